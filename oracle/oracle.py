@@ -1,0 +1,272 @@
+"""ctypes bindings for the CPU oracle libraries.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()``
+and bench.py's CPU-baseline leg as the checker; the product package never
+imports this module.
+
+* :class:`OracleSpace` wraps ``liboracle.so`` -- the C restatement of the
+  reference algorithm (jci_oracle.c).
+* :class:`RefSpace` wraps ``_ref/libjayci_ref.so`` -- the reference's own
+  mpi_source C code compiled unchanged against a single-process GA/MPI
+  stand-in (only present where the reference tree was available at build
+  time; see Makefile).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libjayci_ref.so")
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def build(ref: bool = True) -> None:
+    """Compile the oracle libraries (make -C oracle)."""
+    target = ["all"] if ref else ["liboracle.so"]
+    subprocess.run(["make", "-s", "-C", HERE] + target, check=True)
+
+
+def _load(path):
+    if not os.path.exists(path):
+        build(ref=path == REF_SO)
+    return ctypes.CDLL(path)
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+class OracleSpace:
+    """String space + Slater-rule sigma + Davidson, restated in C."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            lib = _load(ORACLE_SO)
+            lib.jo_space_build.restype = ctypes.c_void_p
+            lib.jo_space_build.argtypes = [ctypes.c_int] * 6
+            lib.jo_space_free.argtypes = [ctypes.c_void_p]
+            lib.jo_space_info.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.jo_strings.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+            lib.jo_eospaces.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+            lib.jo_pq.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.jo_string_index.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+            lib.jo_excitations.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+            lib.jo_hdiag.argtypes = [ctypes.c_void_p] * 4
+            lib.jo_hmatel.restype = ctypes.c_double
+            lib.jo_hmatel.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_longlong] * 2
+            lib.jo_sigma.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+            lib.jo_davidson.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_double] + [ctypes.c_int] * 6 + [
+                                        ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p]
+            lib.jo_symeig.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, ci_aelec, ci_belec, ci_orbs, ndocc=0, nactv=None, xlvl=0):
+        if nactv is None:
+            nactv = ci_orbs - ndocc
+        self.na, self.nb, self.norb = ci_aelec, ci_belec, ci_orbs
+        self.ndocc, self.nactv, self.xlvl = ndocc, nactv, xlvl
+        self.h = self.lib().jo_space_build(ci_aelec, ci_belec, ci_orbs, ndocc,
+                                           nactv, xlvl)
+        if not self.h:
+            raise ValueError("oracle: invalid space")
+        info = np.zeros(6, np.int64)
+        self.lib().jo_space_info(self.h, _ptr(info))
+        (self.nastr, self.nbstr, self.pegrps, self.qegrps, self.npq,
+         self.ndets) = (int(x) for x in info)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib().jo_space_free(self.h)
+            self.h = None
+
+    def strings(self, spin):
+        ns, ne = (self.nastr, self.na) if spin == 0 else (self.nbstr, self.nb)
+        out = np.zeros(ns * ne, np.int32)
+        self.lib().jo_strings(self.h, spin, _ptr(out))
+        return out.reshape(ns, ne)
+
+    def eospaces(self, spin):
+        ng = self.pegrps if spin == 0 else self.qegrps
+        out = np.zeros(5 * ng, np.int32)
+        self.lib().jo_eospaces(self.h, spin, _ptr(out))
+        return out.reshape(ng, 5)
+
+    def pq(self):
+        out = np.zeros(2 * self.npq, np.int32)
+        self.lib().jo_pq(self.h, _ptr(out))
+        return out.reshape(self.npq, 2)
+
+    def excitations(self, spin, nrep, istr, teosp):
+        ns = self.nastr if spin == 0 else self.nbstr
+        out = np.zeros(6 * (ns + 1), np.int32)
+        n = self.lib().jo_excitations(self.h, spin, nrep, istr, teosp, _ptr(out))
+        return out[: 6 * n].reshape(n, 6)
+
+    def hdiag(self, m1, m2):
+        out = np.zeros(self.ndets)
+        self.lib().jo_hdiag(self.h, _ptr(np.ascontiguousarray(m1, float)),
+                            _ptr(np.ascontiguousarray(m2, float)), _ptr(out))
+        return out
+
+    def hmatel(self, m1, m2, i, j):
+        return self.lib().jo_hmatel(self.h, _ptr(m1), _ptr(m2), i, j)
+
+    def sigma(self, m1, m2, V):
+        V = np.ascontiguousarray(np.atleast_2d(V), float)
+        S = np.zeros_like(V)
+        self.lib().jo_sigma(self.h, _ptr(m1), _ptr(m2), V.shape[0], _ptr(V), _ptr(S))
+        return S
+
+    def davidson(self, m1, m2, totcore, maxiter=500, krymin=4, krymax=12,
+                 nroots=1, prediagr=1, refdim=8, restol=1e-8, init=None):
+        e = np.zeros(nroots)
+        civ = np.zeros((nroots, self.ndets))
+        init_p = None
+        if init is not None:
+            init = np.ascontiguousarray(init, float)
+            init_p = _ptr(init)
+        it = self.lib().jo_davidson(self.h, _ptr(m1), _ptr(m2), totcore, maxiter,
+                                    krymin, krymax, nroots, prediagr, refdim,
+                                    restol, init_p, _ptr(e), _ptr(civ))
+        if it < 0:
+            raise ValueError(f"oracle davidson failed ({it})")
+        return e, civ, it
+
+
+def symeig(a):
+    a = np.array(a, float, order="C")
+    n = a.shape[0]
+    w = np.zeros(n)
+    z = np.zeros((n, n))
+    OracleSpace.lib().jo_symeig(n, _ptr(a), _ptr(w), _ptr(z))
+    return w, z
+
+
+class RefSpace:
+    """The reference's own code (oracle/_ref) driven through ref_harness.c.
+
+    The reference keeps its state in globals, so one RefSpace is live at a
+    time (building a new one replaces the previous space)."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            lib = _load(REF_SO)
+            lib.ref_build_space.argtypes = [ctypes.c_int] * 7
+            lib.ref_pdavidson.argtypes = [ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_double, ctypes.c_double] + \
+                [ctypes.c_int] * 7 + [ctypes.c_double, ctypes.c_char_p, ctypes.c_void_p]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, electrons, orbitals, nfrzc=0, ndocc=0, nactv=None,
+                 nfrzv=0, xlvl=0):
+        if nactv is None:
+            nactv = orbitals - nfrzc - nfrzv - ndocc
+        nd = self.lib().ref_build_space(electrons, orbitals, nfrzc, ndocc, nactv,
+                                        nfrzv, xlvl)
+        if nd < 0:
+            raise ValueError("reference: invalid space")
+        sz = np.zeros(10, np.int32)
+        self.lib().ref_sizes(_ptr(sz))
+        (self.na, self.nb, self.norb, self.nastr, self.nbstr, self.pegrps,
+         self.qegrps, self.npq, self.ndets, self.intorb) = (int(x) for x in sz)
+        self.ndocc, self.nactv, self.xlvl = ndocc, nactv, xlvl
+
+    def strings(self, spin):
+        ns, ne = (self.nastr, self.na) if spin == 0 else (self.nbstr, self.nb)
+        istr = np.zeros(ns * ne, np.int32)
+        b1 = np.zeros(ns, np.int64)
+        vx = np.zeros(2 * ns, np.int32)
+        nv = np.zeros(ns, np.int32)
+        self.lib().ref_get_strings(spin, _ptr(istr), _ptr(b1), _ptr(vx), _ptr(nv))
+        return istr.reshape(ns, ne), b1, vx.reshape(ns, 2), nv
+
+    def eospaces(self, spin):
+        ng = self.pegrps if spin == 0 else self.qegrps
+        out = np.zeros(26 * ng, np.int32)
+        self.lib().ref_get_eospaces(spin, _ptr(out))
+        return out.reshape(ng, 26)
+
+    def pq(self):
+        out = np.zeros(2 * self.npq, np.int32)
+        self.lib().ref_get_pq(_ptr(out))
+        return out.reshape(self.npq, 2)
+
+    def yij_cij(self, spin):
+        ns, ne = (self.nastr, self.na) if spin == 0 else (self.nbstr, self.nb)
+        w = self.norb + 1
+        y = np.zeros(ns * ne * w, np.int32)
+        c = np.zeros(ns * ne * w, np.int32)
+        self.lib().ref_get_yij_cij(spin, _ptr(y), _ptr(c))
+        return y.reshape(ns, ne, w), c.reshape(ns, ne, w)
+
+    def excitations(self, spin, nrep, istr, teosp):
+        ns = self.nastr if spin == 0 else self.nbstr
+        out = np.zeros(6 * (ns + 1), np.int32)
+        n = self.lib().ref_excitations(spin, nrep, istr, teosp, _ptr(out))
+        return out[: 6 * n].reshape(n, 6)
+
+    def wlist(self):
+        out = np.zeros(3 * self.ndets, np.int32)
+        self.lib().ref_get_wlist(_ptr(out))
+        return out.reshape(self.ndets, 3)
+
+    def hdiag(self, m1, m2):
+        out = np.zeros(self.ndets)
+        self.lib().ref_hdiag(_ptr(m1), _ptr(m2), _ptr(out))
+        return out
+
+    def sigma(self, m1, m2, V):
+        V = np.ascontiguousarray(np.atleast_2d(V), float)
+        C = np.zeros_like(V)
+        self.lib().ref_sigma(_ptr(m1), _ptr(m2), V.shape[0], _ptr(V), _ptr(C))
+        return C
+
+    def davidson(self, m1, m2, nucrep, frzcore, maxiter=500, krymin=4,
+                 krymax=12, nroots=1, prediagr=1, refdim=8, restol=1e-8,
+                 printlvl=0, workdir=None):
+        civ = np.zeros((nroots, self.ndets))
+        wd = workdir or tempfile.mkdtemp(prefix="jci_ref_")
+        rc = self.lib().ref_pdavidson(_ptr(m1), _ptr(m2), nucrep, frzcore, printlvl,
+                                      maxiter, krymin, krymax, nroots, prediagr,
+                                      refdim, restol, wd.encode(), _ptr(civ))
+        if rc != 0:
+            raise RuntimeError(f"reference pdavidson returned {rc}")
+        return civ, wd
+
+
+def canonical_excitation(row):
+    """(index, io_hi, io_lo, fo_lo, fo_hi, phase) with the phase adjusted to
+    that pairing; the matrix element permx[(io0 fo0|io1 fo1)-(io0 fo1|io1 fo0)]
+    is invariant under this normalisation."""
+    idx, i0, i1, f0, f1, p = (int(x) for x in row)
+    if i1 == 0:
+        return (idx, i0, 0, f0, 0, p)
+    if i0 < i1:                       # swap the two (io, fo) pairs jointly
+        i0, i1, f0, f1 = i1, i0, f1, f0
+    if f0 > f1:                       # swapping only the targets flips sign
+        f0, f1, p = f1, f0, -p
+    return (idx, i0, i1, f0, f1, p)
