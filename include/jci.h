@@ -1,0 +1,269 @@
+/*
+ * jci.h -- C ABI of libjci, the B200-native determinant-CI engine.
+ *
+ * Drop-in boundary for the JayCI hot path: the truncated alpha/beta string
+ * space, the direct Slater-rule sigma = H c build and the Davidson
+ * eigensolver around it.  All compute runs on the current CUDA device;
+ * there is no CPU fallback (calls fail with JCI_ERR_NODEVICE / JCI_ERR_CUDA).
+ *
+ * Signatures use plain C types only.  Citations name the reference
+ * interface each entry point replaces (paths within the JayCI project).
+ *
+ * Conventions shared with the reference:
+ *  - orbitals are 1-based; strings are sorted orbital lists;
+ *  - determinants are ordered by (p,q)-group pair, then alpha string, then
+ *    beta string (pdavidson.c:4757 string_info_to_determinant_fast);
+ *  - integrals are packed as in moindex.c: moints1[index1e(i,j)-1],
+ *    moints2[index2e(i,j,k,l)-1] with index1e(i,j) = max(i,j)(max-1)/2+min;
+ *  - vectors are stored vector-major: v[k*ndets + i].
+ *
+ * Thread safety: distinct handles may be used from distinct host threads;
+ * one handle must not be used concurrently.  Every call returns a status;
+ * the library never exits the process.
+ */
+#ifndef JCI_H
+#define JCI_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+        JCI_OK = 0,
+        JCI_ERR_ARG = 1,       /* invalid argument */
+        JCI_ERR_SPACE = 2,     /* CI space outside the supported limits */
+        JCI_ERR_NOMEM = 3,     /* host or device allocation failed */
+        JCI_ERR_CUDA = 4,      /* CUDA runtime error */
+        JCI_ERR_NODEVICE = 5,  /* no CUDA device (no CPU fallback exists) */
+        JCI_ERR_IO = 6,        /* file could not be opened / read / written */
+        JCI_ERR_FORMAT = 7,    /* malformed SIFS, namelist or vector file */
+        JCI_ERR_NOCONV = 8,    /* Davidson hit maxiter; results still valid */
+        JCI_ERR_LINALG = 9,    /* subspace eigensolve did not converge */
+        JCI_ERR_TIMEOUT = 10,  /* a bounded device wait expired */
+        JCI_ERR_BUSY = 11,     /* server admission refused (queue full) */
+        JCI_ERR_STATE = 12     /* call out of order (e.g. no integrals set) */
+} jci_status;
+
+enum { JCI_FP64 = 0, JCI_FP32 = 1, JCI_MIXED = 2 };
+
+/* Byte layout of the reference's struct occstr (binarystr.h:6-13). */
+struct jci_occstr {
+        long long byte1;
+        int virtx[2];
+        int nvrtx;
+        int istr[20];
+        int yij[20][200];
+        int cij[20][200];
+};
+
+/* Byte layout of the reference's struct eospace (citruncate.h:9-18). */
+struct jci_eospace {
+        int docc;
+        int actv;
+        int virt;
+        int nstr;
+        int start;
+        int pairs[20];
+        int npairs;
+};
+
+const char *jci_status_string(int status);
+/* Number of visible CUDA devices (0 when the driver has none). */
+int jci_device_count(void);
+
+/* ---------------------------------------------------------------------
+ * Drop-in solve.  Same arguments and meaning as the reference's
+ *   int pdavidson(struct occstr *pstrings, struct eospace *peospace,
+ *                 int pegrps, struct occstr *qstrings,
+ *                 struct eospace *qeospace, int qegrps,
+ *                 int **pq_space_pairs, int num_pq, double *moints1,
+ *                 double *moints2, int aelec, int belec, int intorb,
+ *                 int ndets, double nucrep_e, double frzcore_e,
+ *                 int printlvl, int maxiter, int krymin, int krymax,
+ *                 int nroots, int prediagr, int refdim, double restol,
+ *                 int ga_buffer_len, int nmos, int ndocc, int nactv)
+ * (mpi_source/include/pdavidson.h:9, called at execute_pjayci.c:217).
+ * The strings, groups and pairs are the ones citrunc produced; only their
+ * istr/nvrtx fields and the group table are read.  Files "civec" (and
+ * "ci.restart", "hvvec" when not converged) are written to the current
+ * directory in the reference's format (mpi_utilities.c:353).  ga_buffer_len
+ * is accepted and ignored (the reference overrides it too,
+ * pdavidson.c:1327-1335).  Returns 0 on success, a jci_status otherwise.
+ * --------------------------------------------------------------------- */
+int jci_pdavidson(struct jci_occstr *pstrings, struct jci_eospace *peospace,
+                  int pegrps, struct jci_occstr *qstrings,
+                  struct jci_eospace *qeospace, int qegrps,
+                  int **pq_space_pairs, int num_pq, double *moints1,
+                  double *moints2, int aelec, int belec, int intorb,
+                  int ndets, double nucrep_e, double frzcore_e, int printlvl,
+                  int maxiter, int krymin, int krymax, int nroots,
+                  int prediagr, int refdim, double restol, int ga_buffer_len,
+                  int nmos, int ndocc, int nactv);
+
+/* ---------------------------------------------------------------------
+ * String space handle.
+ * --------------------------------------------------------------------- */
+typedef struct jci_space jci_space;
+
+/* Build the truncated alpha/beta string space, replacing citrunc
+ * (citruncate.c:55, citruncate.h:74) with the electron/orbital counts of
+ * the &general namelist.  Limits are the reference's
+ * (execute_pjayci.c:96-153): ci alpha/beta electrons <= 20, CI orbitals
+ * <= 200, ndocc + nactv <= 64. */
+jci_status jci_space_create(int electrons, int orbitals, int nfrzc,
+                            int ndocc, int nactv, int nfrzv, int xlvl,
+                            jci_space **out);
+void jci_space_destroy(jci_space *s);
+
+/* out[10] = {ci_aelec, ci_belec, ci_orbs, nastr, nbstr, pegrps, qegrps,
+ *            num_pq, ndets, intorb} (execute_pjayci.c:157-170). */
+jci_status jci_space_sizes(const jci_space *s, long long *out);
+/* Sorted orbital lists, nstr x nelec, in the order of
+ * generate_string_list (citruncate.c:3971). */
+jci_status jci_space_strings(const jci_space *s, int spin, int *istr);
+/* Per group [docc, actv, virt, nstr, start] (allocate_eospace_array,
+ * citruncate.c:121, counts filled by generate_string_list). */
+jci_status jci_space_eospaces(const jci_space *s, int spin, int *out);
+/* Valid (p,q) group pairs, num_pq x 2 (compute_detnum, citruncate.c:414). */
+jci_status jci_space_pq(const jci_space *s, int *out);
+/* Address of a sorted orbital list, or -1 (occstr2address,
+ * citruncate.c:4093; str_adrfind, straddress.c:48). */
+jci_status jci_space_string_index(const jci_space *s, int spin,
+                                  const int *orbs, int *index);
+/* Single (nrep=1) / double (nrep=2) replacements of string istr landing in
+ * group teosp (generate_single_excitations / generate_double_excitations,
+ * citruncate.c:755,799).  Entries [index, io0, io1, fo0, fo1, permx];
+ * *count receives the number written (out must hold the maximum). */
+jci_status jci_space_excitations(const jci_space *s, int spin, int nrep,
+                                 int istr, int teosp, int *out, int *count);
+
+/* Upload integrals for this space (packed as moindex.c; norb = CI
+ * orbitals) and the core energies (readmointegrals, ioutil.c:416).
+ * Builds the integral-dependent device tables. */
+jci_status jci_set_integrals(jci_space *s, const double *moints1,
+                             const double *moints2, int norb, double nucrep,
+                             double frzcore);
+
+/* <i|H|i> for every determinant into host memory
+ * (compute_diagonal_iHi, pdavidson.c:1586). */
+jci_status jci_hdiag(jci_space *s, double *out);
+
+/* sigma = H v for nvec host vectors (vector-major, ndets each), replacing
+ * perform_hvispacefast / compute_hv_newvectorfaster (pdavidson.c:4328,
+ * 1778) including the diagonal term (compute_hvc_diagonal_ga, :2105).
+ * precision: JCI_FP64 or JCI_FP32 (FP32 storage and accumulation). */
+jci_status jci_sigma(jci_space *s, int nvec, const double *v, double *sigma,
+                     int precision);
+
+/* Same on device memory: nvec vectors with leading dimension ld (>= ndets,
+ * elements); element type double for JCI_FP64, float for JCI_FP32.  The
+ * work is queued on `stream` (a cudaStream_t, NULL = default stream). */
+jci_status jci_sigma_device(jci_space *s, int nvec, const void *v,
+                            void *sigma, long long ld, int precision,
+                            void *stream);
+
+/* Launch shape the sigma autotuner picked for this space (threads per CTA
+ * and alpha rows staged per pass; both 0 before the first sigma call or on
+ * the multi-group path) and its timed cost in ms per vector.  No reference
+ * counterpart (the reference has no device tuning). */
+jci_status jci_sigma_tuning(const jci_space *s, int precision, int *threads,
+                            int *rows, float *ms);
+
+typedef struct {
+        int maxiter;      /* &dalginfo defaults: 20 */
+        int krymin;       /* 3 */
+        int krymax;       /* 8 */
+        int nroots;       /* 1 */
+        int prediagr;     /* 1 = H over the first refdim dets, 2 = unit
+                           * vectors, 3 = start vectors (init or ci.restart) */
+        int refdim;       /* 3 */
+        double restol;    /* 1e-5 */
+        int precision;    /* JCI_FP64 or JCI_MIXED */
+        double switch_tol;/* mixed: FP32 sigma until ||r|| < switch_tol */
+        int printlvl;
+        int write_files;  /* write civec / ci.restart / hvvec to cwd */
+        int block;        /* 0 = the reference's root-sequential Davidson;
+                           * 1 = block Davidson over all unconverged roots */
+        const double *init; /* prediagr == 3: krymin start vectors, or NULL
+                             * to read "ci.restart" from the cwd */
+} jci_davidson_opts;
+
+typedef struct {
+        int iterations;       /* vectors added (the reference's citer) */
+        int sigma_calls;
+        long long sigma_vectors;
+        double sigma_seconds; /* device time in sigma kernels */
+        double total_seconds;
+        int converged;
+        double rnorm;         /* last residual norm */
+        int fp32_sigma_vectors;
+} jci_davidson_stats;
+
+/* Fill opts with the &dalginfo defaults (readnamelist.f90:85-92). */
+void jci_davidson_defaults(jci_davidson_opts *o);
+
+/* Davidson solve for the lowest nroots (pdavidson.c:39).  energies[nroots]
+ * include nucrep + frzcore; civec (nullable) receives nroots x ndets.
+ * Returns JCI_ERR_NOCONV when maxiter was reached (outputs still set). */
+jci_status jci_davidson(jci_space *s, const jci_davidson_opts *o,
+                        double *energies, double *civec,
+                        jci_davidson_stats *stats);
+
+/* ---------------------------------------------------------------------
+ * Input / output formats.
+ * --------------------------------------------------------------------- */
+
+/* &general namelist (readnamelist.f90:43-44). */
+typedef struct {
+        int electrons, orbitals, nfrozen, ndocc, nactive, xlevel, nfrzvirt;
+        int printlvl, printwvf;
+} jci_general;
+
+/* &dalginfo namelist (readnamelist.f90:45-46, defaults :85-92). */
+typedef struct {
+        int maxiter, krymin, krymax, nroots, prediagr, refdim, buflen;
+        double restol;
+} jci_dalginfo;
+
+/* &gpuinfo namelist (new; absent blocks keep the defaults):
+ * precision (0 fp64, 2 mixed), switchtol, block (0/1), exactrestol.
+ * With exactrestol = 0 (default) restol is rounded as the reference's
+ * f10.5 round trip does (readnamelist.f90:105, ioutil.c:337). */
+typedef struct {
+        int precision;
+        double switch_tol;
+        int block;
+        int exact_restol;
+} jci_gpuinfo;
+
+/* Read jayci.in-style namelists (readgeninput / readdaiinput,
+ * ioutil.c:313,367).  Any of the output pointers may be NULL. */
+jci_status jci_read_namelists(const char *path, jci_general *g,
+                              jci_dalginfo *d, jci_gpuinfo *u);
+
+/* Read a SIFS integral file (readmoints.f90:21 with colib sifrsh/sifd2):
+ * moints1 (m1cap doubles) and moints2 (m2cap doubles) are zeroed and
+ * filled in index1e/index2e packing; *nbft receives the orbital count,
+ * *nucrep energy(1) of header 2, *frzcore the H1 core energy. */
+jci_status jci_read_moints(const char *path, double *moints1, long long m1cap,
+                           double *moints2, long long m2cap, int *nbft,
+                           double *nucrep, double *frzcore);
+
+/* Write a single-symmetry SIFS file with the given packed integrals
+ * (colib sifwh / sifew1 / sifew2 layout, 8-bit labels, fsplit = 1). */
+jci_status jci_write_moints(const char *path, int nbft,
+                            const double *moints1, const double *moints2,
+                            double nucrep, double frzcore);
+
+/* Unformatted vector files "civec" / "ci.restart" / "hvvec":
+ * int32 dim, int32 len, dim*len float64 (mpi_utilities.c:353,430). */
+jci_status jci_write_vectors(const char *path, int dim, int len,
+                             const double *v);
+jci_status jci_read_vectors(const char *path, int dim, int len, double *v);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,308 @@
+"""jayci_b200 -- Python host mirror of the libjci C ABI (include/jci.h).
+
+The engine itself is the in-tree shared library ``libjci.so`` (C++ host code
+plus sm_100a CUDA kernels).  This module binds it with ctypes and mirrors the
+reference's interface for the determinant-CI hot path:
+
+* :class:`Space` -- ``citrunc`` (string space), ``generate_*_excitations``,
+  ``compute_diagonal_iHi``, sigma (``perform_hvispacefast``) and the
+  Davidson solve (``pdavidson``);
+* :func:`read_moints` / :func:`write_moints` -- SIFS integrals
+  (``readmoints.f90``);
+* :func:`read_namelists` -- ``jayci.in`` (``readgeninput`` /
+  ``readdaiinput``);
+* :func:`write_vectors` / :func:`read_vectors` -- civec / ci.restart.
+
+There is no CPU fallback: every call fails loudly (:class:`JciError`) when
+the library or a CUDA device is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libjci.so")
+
+FP64, FP32, MIXED = 0, 1, 2
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "CI space outside the supported limits",
+          3: "out of memory", 4: "CUDA runtime error", 5: "no CUDA device",
+          6: "file I/O error", 7: "malformed input file", 8: "not converged",
+          9: "subspace eigensolve failed", 10: "bounded device wait expired",
+          11: "server admission refused", 12: "call out of order"}
+NOCONV = 8
+
+
+class JciError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        super().__init__(f"libjci {what}: {STATUS.get(status, status)} ({status})")
+
+
+class DavidsonOpts(ctypes.Structure):
+    _fields_ = [("maxiter", ctypes.c_int), ("krymin", ctypes.c_int),
+                ("krymax", ctypes.c_int), ("nroots", ctypes.c_int),
+                ("prediagr", ctypes.c_int), ("refdim", ctypes.c_int),
+                ("restol", ctypes.c_double), ("precision", ctypes.c_int),
+                ("switch_tol", ctypes.c_double), ("printlvl", ctypes.c_int),
+                ("write_files", ctypes.c_int), ("block", ctypes.c_int),
+                ("init", ctypes.c_void_p)]
+
+
+class DavidsonStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("sigma_calls", ctypes.c_int),
+                ("sigma_vectors", ctypes.c_longlong), ("sigma_seconds", ctypes.c_double),
+                ("total_seconds", ctypes.c_double), ("converged", ctypes.c_int),
+                ("rnorm", ctypes.c_double), ("fp32_sigma_vectors", ctypes.c_int)]
+
+
+class General(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int) for k in ("electrons", "orbitals", "nfrozen", "ndocc",
+                                           "nactive", "xlevel", "nfrzvirt", "printlvl",
+                                           "printwvf")]
+
+
+class Dalginfo(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int) for k in ("maxiter", "krymin", "krymax", "nroots",
+                                           "prediagr", "refdim", "buflen")] + \
+        [("restol", ctypes.c_double)]
+
+
+class Gpuinfo(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("switch_tol", ctypes.c_double),
+                ("block", ctypes.c_int), ("exact_restol", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libjci.so (building it first if it is absent)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            from . import build as _b
+            _b.build()
+        L = ctypes.CDLL(LIBPATH)
+        vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.jci_status_string.restype = ctypes.c_char_p
+        L.jci_space_create.argtypes = [ip] * 7 + [ctypes.POINTER(vp)]
+        L.jci_space_destroy.argtypes = [vp]
+        L.jci_space_sizes.argtypes = [vp, vp]
+        L.jci_space_strings.argtypes = [vp, ip, vp]
+        L.jci_space_eospaces.argtypes = [vp, ip, vp]
+        L.jci_space_pq.argtypes = [vp, vp]
+        L.jci_space_string_index.argtypes = [vp, ip, vp, ctypes.POINTER(ip)]
+        L.jci_space_excitations.argtypes = [vp, ip, ip, ip, ip, vp, ctypes.POINTER(ip)]
+        L.jci_set_integrals.argtypes = [vp, vp, vp, ip, dp, dp]
+        L.jci_hdiag.argtypes = [vp, vp]
+        L.jci_sigma.argtypes = [vp, ip, vp, vp, ip]
+        L.jci_sigma_device.argtypes = [vp, ip, vp, vp, ctypes.c_longlong, ip, vp]
+        L.jci_davidson_defaults.argtypes = [ctypes.POINTER(DavidsonOpts)]
+        L.jci_davidson.argtypes = [vp, ctypes.POINTER(DavidsonOpts), vp, vp,
+                                   ctypes.POINTER(DavidsonStats)]
+        L.jci_sigma_tuning.argtypes = [vp, ip, ctypes.POINTER(ip), ctypes.POINTER(ip),
+                                       ctypes.POINTER(ctypes.c_float)]
+        L.jci_read_namelists.argtypes = [ctypes.c_char_p, vp, vp, vp]
+        L.jci_read_moints.argtypes = [ctypes.c_char_p, vp, ctypes.c_longlong, vp,
+                                      ctypes.c_longlong, ctypes.POINTER(ip),
+                                      ctypes.POINTER(dp), ctypes.POINTER(dp)]
+        L.jci_write_moints.argtypes = [ctypes.c_char_p, ip, vp, vp, dp, dp]
+        L.jci_write_vectors.argtypes = [ctypes.c_char_p, ip, ip, vp]
+        L.jci_read_vectors.argtypes = [ctypes.c_char_p, ip, ip, vp]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _check(st, what):
+    if st != 0:
+        raise JciError(st, what)
+
+
+def device_count() -> int:
+    return lib().jci_device_count()
+
+
+@dataclass
+class SolveResult:
+    energies: np.ndarray
+    civec: np.ndarray | None
+    stats: DavidsonStats
+    converged: bool
+
+
+class Space:
+    """Truncated alpha/beta CI string space (citrunc, citruncate.c:55) with
+    its device tables.  Arguments are the &general namelist values."""
+
+    def __init__(self, electrons, orbitals, nfrozen=0, ndocc=0, nactive=None,
+                 nfrzvirt=0, xlevel=0):
+        if nactive is None:
+            nactive = orbitals - nfrozen - nfrzvirt - ndocc
+        h = ctypes.c_void_p()
+        _check(lib().jci_space_create(electrons, orbitals, nfrozen, ndocc, nactive,
+                                      nfrzvirt, xlevel, ctypes.byref(h)), "space_create")
+        self.h = h
+        sz = np.zeros(10, np.int64)
+        lib().jci_space_sizes(h, _p(sz))
+        (self.na, self.nb, self.norb, self.nastr, self.nbstr, self.pegrps,
+         self.qegrps, self.npq, self.ndets, self.intorb) = (int(x) for x in sz)
+        self.ndocc, self.nactv, self.xlvl = ndocc, nactive, xlevel
+
+    def close(self):
+        if getattr(self, "h", None):
+            try:
+                lib().jci_space_destroy(self.h)
+            except Exception:  # interpreter shutdown
+                pass
+            self.h = None
+
+    __del__ = close
+
+    def strings(self, spin):
+        ns, ne = (self.nastr, self.na) if spin == 0 else (self.nbstr, self.nb)
+        out = np.zeros(ns * ne, np.int32)
+        _check(lib().jci_space_strings(self.h, spin, _p(out)), "strings")
+        return out.reshape(ns, ne)
+
+    def eospaces(self, spin):
+        ng = self.pegrps if spin == 0 else self.qegrps
+        out = np.zeros(5 * ng, np.int32)
+        _check(lib().jci_space_eospaces(self.h, spin, _p(out)), "eospaces")
+        return out.reshape(ng, 5)
+
+    def pq(self):
+        out = np.zeros(2 * self.npq, np.int32)
+        _check(lib().jci_space_pq(self.h, _p(out)), "pq")
+        return out.reshape(self.npq, 2)
+
+    def string_index(self, spin, orbs):
+        o = np.ascontiguousarray(orbs, np.int32)
+        idx = ctypes.c_int()
+        _check(lib().jci_space_string_index(self.h, spin, _p(o), ctypes.byref(idx)),
+               "string_index")
+        return idx.value
+
+    def excitations(self, spin, nrep, istr, teosp):
+        ns = self.nastr if spin == 0 else self.nbstr
+        out = np.zeros(6 * (ns + 1), np.int32)
+        n = ctypes.c_int()
+        _check(lib().jci_space_excitations(self.h, spin, nrep, istr, teosp, _p(out),
+                                           ctypes.byref(n)), "excitations")
+        return out[: 6 * n.value].reshape(n.value, 6)
+
+    def set_integrals(self, moints1, moints2, nucrep=0.0, frzcore=0.0):
+        self._m1 = np.ascontiguousarray(moints1, np.float64)
+        self._m2 = np.ascontiguousarray(moints2, np.float64)
+        _check(lib().jci_set_integrals(self.h, _p(self._m1), _p(self._m2), self.norb,
+                                       nucrep, frzcore), "set_integrals")
+
+    def hdiag(self):
+        out = np.zeros(self.ndets)
+        _check(lib().jci_hdiag(self.h, _p(out)), "hdiag")
+        return out
+
+    def sigma(self, v, precision=FP64):
+        v = np.ascontiguousarray(np.atleast_2d(v), np.float64)
+        out = np.zeros_like(v)
+        _check(lib().jci_sigma(self.h, v.shape[0], _p(v), _p(out), precision), "sigma")
+        return out
+
+    def sigma_device(self, v_ptr, s_ptr, nvec, ld, precision=FP64, stream=None):
+        """sigma on device buffers (e.g. torch tensors' data_ptr())."""
+        _check(lib().jci_sigma_device(self.h, nvec, ctypes.c_void_p(v_ptr),
+                                      ctypes.c_void_p(s_ptr), ld, precision,
+                                      ctypes.c_void_p(stream or 0)), "sigma_device")
+
+    def sigma_tuning(self, precision=FP64):
+        """(threads per CTA, staged rows, ms per vector) chosen by the autotuner."""
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        _check(lib().jci_sigma_tuning(self.h, precision, ctypes.byref(a), ctypes.byref(b),
+                                      ctypes.byref(c)), "sigma_tuning")
+        return a.value, b.value, c.value
+
+    def davidson(self, maxiter=500, krymin=4, krymax=12, nroots=1, prediagr=1,
+                 refdim=8, restol=1e-8, precision=FP64, switch_tol=1e-4,
+                 block=False, printlvl=0, write_files=False, init=None,
+                 want_vectors=True) -> SolveResult:
+        o = DavidsonOpts()
+        lib().jci_davidson_defaults(ctypes.byref(o))
+        o.maxiter, o.krymin, o.krymax, o.nroots = maxiter, krymin, krymax, nroots
+        o.prediagr, o.refdim, o.restol = prediagr, refdim, restol
+        o.precision, o.switch_tol, o.block = precision, switch_tol, int(block)
+        o.printlvl, o.write_files = printlvl, int(write_files)
+        if init is not None:
+            init = np.ascontiguousarray(init, np.float64)
+            o.init = init.ctypes.data
+        e = np.zeros(nroots)
+        civ = np.zeros((nroots, self.ndets)) if want_vectors else None
+        st = DavidsonStats()
+        r = lib().jci_davidson(self.h, ctypes.byref(o), _p(e),
+                               _p(civ) if civ is not None else None, ctypes.byref(st))
+        if r not in (0, NOCONV):
+            raise JciError(r, "davidson")
+        return SolveResult(e, civ, st, r == 0)
+
+
+def read_namelists(path):
+    g, d, u = General(), Dalginfo(), Gpuinfo()
+    _check(lib().jci_read_namelists(str(path).encode(), ctypes.byref(g), ctypes.byref(d),
+                                    ctypes.byref(u)), "read_namelists")
+    return g, d, u
+
+
+def moint_sizes(norb):
+    m1 = norb * (norb + 1) // 2
+    return m1, m1 * (m1 + 1) // 2
+
+
+def sifs_nbft(path):
+    """Orbital count from SIFS header 1 (seven INTEGER*8, readmoints.f90:101)."""
+    try:
+        with open(path, "rb") as f:
+            head = f.read(4 + 56)
+    except OSError:
+        raise JciError(6, "read_moints") from None
+    if len(head) < 60:
+        raise JciError(7, "read_moints")
+    return int(np.frombuffer(head[4:60], np.int64)[3])
+
+
+def read_moints(path):
+    """SIFS integrals -> (moints1, moints2, nbft, nucrep, frzcore)."""
+    m1len, m2len = moint_sizes(sifs_nbft(path))
+    m1 = np.zeros(m1len)
+    m2 = np.zeros(m2len)
+    nb, en, fc = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+    _check(lib().jci_read_moints(str(path).encode(), _p(m1), m1len, _p(m2), m2len,
+                                 ctypes.byref(nb), ctypes.byref(en), ctypes.byref(fc)),
+           "read_moints")
+    a, b = moint_sizes(nb.value)
+    return m1[:a].copy(), m2[:b].copy(), nb.value, en.value, fc.value
+
+
+def write_moints(path, nbft, moints1, moints2, nucrep, frzcore=0.0):
+    m1 = np.ascontiguousarray(moints1, np.float64)
+    m2 = np.ascontiguousarray(moints2, np.float64)
+    _check(lib().jci_write_moints(str(path).encode(), nbft, _p(m1), _p(m2), nucrep, frzcore),
+           "write_moints")
+
+
+def write_vectors(path, v):
+    v = np.ascontiguousarray(np.atleast_2d(v), np.float64)
+    _check(lib().jci_write_vectors(str(path).encode(), v.shape[0], v.shape[1], _p(v)),
+           "write_vectors")
+
+
+def read_vectors(path, dim, length):
+    v = np.zeros((dim, length))
+    _check(lib().jci_read_vectors(str(path).encode(), dim, length, _p(v)), "read_vectors")
+    return v

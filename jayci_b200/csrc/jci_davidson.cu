@@ -1,0 +1,835 @@
+// jci_davidson.cu -- Davidson eigensolver with every vector resident on the
+// device (the reference keeps V, C, N, R, X, D in Global Arrays,
+// pdavidson.c:111-135).
+//
+// Two schedules share the kernels below:
+//  * block = 0: the reference's root-sequential algorithm (pdavidson.c:39):
+//    one correction vector per iteration for the current root, classical
+//    Gram-Schmidt in one pass (:4086), collapse to krymin Ritz vectors when
+//    the space reaches krymax (:4821).  The subspace matrix is V_i . C_j for
+//    i >= j (make_subspacehmat_ga :4053 read through dsyevr's upper
+//    triangle), the residual r = sum_i y_i (c_i - theta v_i) (:3802), the
+//    correction t = r / (theta - D) (:3773).  After a collapse the sigma
+//    vectors are rotated with the same Ritz coefficients instead of being
+//    recomputed (identical in exact arithmetic).
+//  * block = 1: block Davidson over all unconverged roots (one correction
+//    per root per iteration, two Gram-Schmidt passes), so a sigma launch
+//    processes several vectors and every root converges together.
+// Precision: JCI_FP64, or JCI_MIXED = FP32 sigma (FP32 storage and
+// accumulation) until the largest residual norm drops below switch_tol,
+// then every sigma vector of the current basis is recomputed in FP64 and
+// the iterations continue in FP64.  Basis vectors, Gram-Schmidt, residuals,
+// the Hdiag preconditioner, the Rayleigh-Ritz eigensolve and the energies
+// are FP64 throughout.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "jci_kernels.cuh"
+
+namespace jci {
+
+constexpr int kMaxKry = 64;
+constexpr int kDotBlocks = 296;  // 2 x 148 SMs
+
+struct DavidsonBuffers {
+    long long ld = 0;
+    int cap = 0;             // vectors allocated in V and C
+    double *V = nullptr, *C = nullptr, *X = nullptr, *Y2 = nullptr;
+    double *r = nullptr, *t = nullptr;
+    float *v32 = nullptr, *s32 = nullptr;
+    int cap32 = 0;
+    double *partial = nullptr;   // kDotBlocks x kMaxKry
+    double *dots = nullptr;      // kMaxKry
+    double *G = nullptr, *evec = nullptr, *eval = nullptr;
+    double *coef = nullptr;      // 2 x kMaxKry x kMaxKry
+};
+
+void davidson_free(DeviceState *d) {
+    DavidsonBuffers *b = d->dav;
+    if (!b) return;
+    void *p[] = {b->V, b->C, b->X, b->Y2, b->r, b->t, b->v32, b->s32, b->partial,
+                 b->dots, b->G, b->evec, b->eval, b->coef};
+    for (void *q : p) cudaFree(q);
+    delete b;
+    d->dav = nullptr;
+}
+
+// ---- kernels -------------------------------------------------------------
+
+// partial[b*m + i] = sum over this block's slice of X_i . y
+__global__ void __launch_bounds__(256) k_dots(const double *__restrict__ X, int m, long long ld,
+                                              const double *__restrict__ y, long long n,
+                                              double *partial) {
+    __shared__ double red[8][kMaxKry];
+    long long chunk = (n + gridDim.x - 1) / gridDim.x;
+    long long lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = 0; i < m; i++) {
+        const double *x = X + i * ld;
+        double s = 0.0;
+        for (long long k = lo + threadIdx.x; k < hi; k += blockDim.x) s += x[k] * y[k];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) red[warp][i] = s;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        double s = 0.0;
+        for (int w = 0; w < 8; w++) s += red[w][i];
+        partial[blockIdx.x * kMaxKry + i] = s;
+    }
+}
+
+// out[i] = sum_b partial[b][i] in a fixed order (bitwise reproducible).
+__global__ void k_dots_finish(const double *__restrict__ partial, int nb, int m, double *out) {
+    int i = blockIdx.x;
+    __shared__ double red[32];
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nb; b += 32) s += partial[b * kMaxKry + i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) red[0] = s;
+    __syncwarp();
+    if (threadIdx.x == 0 && i < m) out[i] = red[0];
+}
+
+// out[k] = sum_i a[i] X_i[k] + sum_i b[i] Y_i[k]   (coefficients on device)
+__global__ void k_lincomb(double *__restrict__ out, long long n, long long ld,
+                          const double *__restrict__ X, const double *__restrict__ a, int mx,
+                          const double *__restrict__ Y, const double *__restrict__ b, int my) {
+    __shared__ double ca[kMaxKry], cb[kMaxKry];
+    for (int i = threadIdx.x; i < mx; i += blockDim.x) ca[i] = a[i];
+    for (int i = threadIdx.x; i < my; i += blockDim.x) cb[i] = b[i];
+    __syncthreads();
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int i = 0; i < mx; i++) s += ca[i] * X[i * ld + k];
+        for (int i = 0; i < my; i++) s += cb[i] * Y[i * ld + k];
+        out[k] = s;
+    }
+}
+
+// t -= sum_i ov[i] X_i ; used by classical Gram-Schmidt
+__global__ void k_orth_update(double *__restrict__ t, long long n, long long ld,
+                              const double *__restrict__ X, const double *__restrict__ ov,
+                              int m) {
+    __shared__ double c[kMaxKry];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) c[i] = ov[i];
+    __syncthreads();
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        double s = t[k];
+        for (int i = 0; i < m; i++) s -= c[i] * X[i * ld + k];
+        t[k] = s;
+    }
+}
+
+// t = r / (theta - D)   (generate_newvector, pdavidson.c:3773)
+__global__ void k_precond(const double *__restrict__ r, const double *__restrict__ D,
+                          double theta, double *__restrict__ t, long long n) {
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        double den = theta - D[k];
+        // the reference divides without a guard; an exact zero would give inf
+        if (fabs(den) < 1e-14) den = den < 0 ? -1e-14 : 1e-14;
+        t[k] = r[k] / den;
+    }
+}
+
+// x *= 1 / sqrt(*nrm2)
+__global__ void k_normalize(double *__restrict__ x, long long n, const double *__restrict__ nrm2) {
+    double s = 1.0 / sqrt(*nrm2);
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x)
+        x[k] *= s;
+}
+
+__global__ void k_d2f(const double *__restrict__ in, float *__restrict__ out, long long n,
+                      long long ldi, long long ldo, int m) {
+    for (int c = 0; c < m; c++)
+        for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+             k += (long long)gridDim.x * blockDim.x)
+            out[c * ldo + k] = (float)in[c * ldi + k];
+}
+
+__global__ void k_f2d(const float *__restrict__ in, double *__restrict__ out, long long n,
+                      long long ldi, long long ldo, int m) {
+    for (int c = 0; c < m; c++)
+        for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+             k += (long long)gridDim.x * blockDim.x)
+            out[c * ldo + k] = (double)in[c * ldi + k];
+}
+
+// Cyclic Jacobi eigensolve of the m x m symmetric matrix held in the lower
+// triangle of G (G[i*ldg + j], i >= j), one warp.  Eigenvalues ascending in
+// w; eigenvector k in Y[k*ldg + .], sign fixed so that its largest-magnitude
+// component is positive.  info = number of sweeps, or -1 if not converged.
+__global__ void k_jacobi(const double *__restrict__ G, int m, int ldg, double *w, double *Y,
+                         int *info) {
+    extern __shared__ double sm[];
+    double *A = sm;                 // m x (m+1)
+    double *Vm = sm + m * (m + 1);  // m x (m+1)
+    const int lane = threadIdx.x, st = m + 1;
+    for (int i = lane; i < m * m; i += 32) {
+        int r = i / m, c = i % m;
+        A[r * st + c] = r >= c ? G[r * ldg + c] : G[c * ldg + r];
+        Vm[r * st + c] = r == c ? 1.0 : 0.0;
+    }
+    __syncwarp();
+    int sweep = 0, conv = 0;
+    for (; sweep < 60; sweep++) {
+        double off = 0.0, dia = 0.0;
+        for (int i = lane; i < m * m; i += 32) {
+            int r = i / m, c = i % m;
+            double x = A[r * st + c];
+            if (r != c) off += x * x;
+            else dia += x * x;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            off += __shfl_xor_sync(0xffffffffu, off, o);
+            dia += __shfl_xor_sync(0xffffffffu, dia, o);
+        }
+        if (off <= 1e-30 * fmax(dia, 1e-300)) {
+            conv = 1;
+            break;
+        }
+        for (int p = 0; p < m - 1; p++)
+            for (int q = p + 1; q < m; q++) {
+                double apq = A[p * st + q];
+                double app = A[p * st + p], aqq = A[q * st + q];
+                if (fabs(apq) <= 1e-300 || fabs(apq) <= 1e-18 * sqrt(fabs(app * aqq))) continue;
+                double th = (aqq - app) / (2.0 * apq);
+                double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+                double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                __syncwarp();
+                for (int k = lane; k < m; k += 32) {
+                    double akp = A[k * st + p], akq = A[k * st + q];
+                    A[k * st + p] = c * akp - s * akq;
+                    A[k * st + q] = s * akp + c * akq;
+                }
+                __syncwarp();
+                for (int k = lane; k < m; k += 32) {
+                    double apk = A[p * st + k], aqk = A[q * st + k];
+                    A[p * st + k] = c * apk - s * aqk;
+                    A[q * st + k] = s * apk + c * aqk;
+                    double vkp = Vm[k * st + p], vkq = Vm[k * st + q];
+                    Vm[k * st + p] = c * vkp - s * vkq;
+                    Vm[k * st + q] = s * vkp + c * vkq;
+                }
+                __syncwarp();
+            }
+    }
+    __syncwarp();
+    if (lane == 0) {
+        // selection order by eigenvalue (stable for equal values)
+        int ord[kMaxKry];
+        for (int i = 0; i < m; i++) ord[i] = i;
+        for (int i = 1; i < m; i++) {
+            int x = ord[i], j = i;
+            while (j > 0 && A[ord[j - 1] * st + ord[j - 1]] > A[x * st + x]) {
+                ord[j] = ord[j - 1];
+                j--;
+            }
+            ord[j] = x;
+        }
+        for (int k = 0; k < m; k++) {
+            int c = ord[k];
+            w[k] = A[c * st + c];
+            double big = 0.0;
+            int bi = 0;
+            for (int i = 0; i < m; i++)
+                if (fabs(Vm[i * st + c]) > big + 1e-14) {
+                    big = fabs(Vm[i * st + c]);
+                    bi = i;
+                }
+            double sg = Vm[bi * st + c] < 0 ? -1.0 : 1.0;
+            for (int i = 0; i < m; i++) Y[k * ldg + i] = sg * Vm[i * st + c];
+        }
+        *info = conv ? sweep : -1;
+    }
+}
+
+// ---- host driver ---------------------------------------------------------
+
+static unsigned grid_for(long long n) {
+    long long g = (n + 255) / 256;
+    return (unsigned)std::max(1LL, std::min(g, 148LL * 8));
+}
+
+struct Ctx {
+    jci_space *s;
+    DeviceState *d;
+    DavidsonBuffers *b;
+    cudaStream_t st;
+    long long n, ld;
+    int *d_info = nullptr;
+    double sigma_ms = 0.0;
+    int sigma_calls = 0;
+    long long sigma_vecs = 0;
+    int fp32_vecs = 0;
+};
+
+static jci_status ensure_buffers(Ctx &c, int cap, bool mixed, int maxnew) {
+    DeviceState *d = c.d;
+    if (!d->dav) d->dav = new DavidsonBuffers();
+    DavidsonBuffers *b = d->dav;
+    c.b = b;
+    long long ld = (c.n + 31) / 32 * 32;
+    if (b->ld != ld || b->cap < cap) {
+        void *p[] = {b->V, b->C, b->X, b->r, b->t};
+        for (void *q : p) cudaFree(q);
+        b->ld = ld;
+        b->cap = cap;
+        JCI_CUDA(cudaMalloc(&b->V, (size_t)cap * ld * sizeof(double)));
+        JCI_CUDA(cudaMalloc(&b->C, (size_t)cap * ld * sizeof(double)));
+        JCI_CUDA(cudaMalloc(&b->X, (size_t)cap * ld * sizeof(double)));
+        JCI_CUDA(cudaMalloc(&b->r, (size_t)ld * sizeof(double)));
+        JCI_CUDA(cudaMalloc(&b->t, (size_t)ld * sizeof(double)));
+        if (!b->partial) {
+            JCI_CUDA(cudaMalloc(&b->partial, kDotBlocks * kMaxKry * sizeof(double)));
+            JCI_CUDA(cudaMalloc(&b->dots, kMaxKry * sizeof(double)));
+            JCI_CUDA(cudaMalloc(&b->G, kMaxKry * kMaxKry * sizeof(double)));
+            JCI_CUDA(cudaMalloc(&b->evec, kMaxKry * kMaxKry * sizeof(double)));
+            JCI_CUDA(cudaMalloc(&b->eval, kMaxKry * sizeof(double)));
+            JCI_CUDA(cudaMalloc(&b->coef, 2 * kMaxKry * kMaxKry * sizeof(double)));
+        }
+    }
+    if (mixed && (b->cap32 < maxnew || !b->v32)) {
+        cudaFree(b->v32);
+        cudaFree(b->s32);
+        b->cap32 = maxnew;
+        JCI_CUDA(cudaMalloc(&b->v32, (size_t)maxnew * ld * sizeof(float)));
+        JCI_CUDA(cudaMalloc(&b->s32, (size_t)maxnew * ld * sizeof(float)));
+    }
+    c.ld = ld;
+    JCI_CUDA(cudaMemsetAsync(b->V, 0, (size_t)cap * ld * sizeof(double), c.st));
+    JCI_CUDA(cudaMemsetAsync(b->C, 0, (size_t)cap * ld * sizeof(double), c.st));
+    return JCI_OK;
+}
+
+// C[i0 .. i0+m) = H V[i0 .. i0+m) in the requested precision
+static jci_status sigma_block(Ctx &c, int i0, int m, bool fp32) {
+    DavidsonBuffers *b = c.b;
+    auto t0 = std::chrono::steady_clock::now();
+    cudaEvent_t e0 = c.d->ev0, e1 = c.d->ev1;
+    jci_status r;
+    if (fp32) {
+        for (int k0 = 0; k0 < m; k0 += b->cap32) {
+            int mm = std::min(b->cap32, m - k0);
+            k_d2f<<<grid_for(c.n), 256, 0, c.st>>>(b->V + (i0 + k0) * c.ld, b->v32, c.n, c.ld,
+                                                   c.ld, mm);
+            if ((r = device_sigma(c.s, mm, b->v32, b->s32, c.ld, JCI_FP32, c.st))) return r;
+            float ms = 0.f;
+            JCI_CUDA(cudaEventSynchronize(e1));
+            JCI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            c.sigma_ms += ms;
+            k_f2d<<<grid_for(c.n), 256, 0, c.st>>>(b->s32, b->C + (i0 + k0) * c.ld, c.n, c.ld,
+                                                   c.ld, mm);
+        }
+        c.fp32_vecs += m;
+    } else {
+        if ((r = device_sigma(c.s, m, b->V + i0 * c.ld, b->C + i0 * c.ld, c.ld, JCI_FP64,
+                              c.st)))
+            return r;
+        float ms = 0.f;
+        JCI_CUDA(cudaEventSynchronize(e1));
+        JCI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        c.sigma_ms += ms;
+    }
+    (void)t0;
+    c.sigma_calls++;
+    c.sigma_vecs += m;
+    JCI_CUDA(cudaGetLastError());
+    return JCI_OK;
+}
+
+// dots[i] = X_i . y for i < m (device), optionally copied to host
+static jci_status dots(Ctx &c, const double *X, int m, const double *y, double *host) {
+    k_dots<<<kDotBlocks, 256, 0, c.st>>>(X, m, c.ld, y, c.n, c.b->partial);
+    k_dots_finish<<<m, 32, 0, c.st>>>(c.b->partial, kDotBlocks, m, c.b->dots);
+    if (host) {
+        JCI_CUDA(cudaMemcpyAsync(host, c.b->dots, m * sizeof(double), cudaMemcpyDeviceToHost,
+                                 c.st));
+        JCI_CUDA(cudaStreamSynchronize(c.st));
+    }
+    JCI_CUDA(cudaGetLastError());
+    return JCI_OK;
+}
+
+// G[i][j] = V_i . C_j for rows i in [r0, r1) and j <= i (lower triangle)
+static jci_status gram_rows(Ctx &c, int r0, int r1, std::vector<double> &G) {
+    std::vector<double> h(kMaxKry);
+    for (int i = r0; i < r1; i++) {
+        jci_status r = dots(c, c.b->C, i + 1, c.b->V + i * c.ld, h.data());
+        if (r) return r;
+        for (int j = 0; j <= i; j++) G[i * kMaxKry + j] = h[j];
+    }
+    return JCI_OK;
+}
+
+static jci_status rayleigh_ritz(Ctx &c, int m, const std::vector<double> &G,
+                                std::vector<double> &w, std::vector<double> &Y) {
+    DavidsonBuffers *b = c.b;
+    JCI_CUDA(cudaMemcpyAsync(b->G, G.data(), kMaxKry * kMaxKry * sizeof(double),
+                             cudaMemcpyHostToDevice, c.st));
+    size_t smem = 2 * (size_t)m * (m + 1) * sizeof(double);
+    static bool attr_set = false;
+    if (!attr_set) {
+        JCI_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(2 * kMaxKry * (kMaxKry + 1) * sizeof(double))));
+        attr_set = true;
+    }
+    k_jacobi<<<1, 32, smem, c.st>>>(b->G, m, kMaxKry, b->eval, b->evec, c.d_info);
+    int info = 0;
+    JCI_CUDA(cudaMemcpyAsync(w.data(), b->eval, m * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+    JCI_CUDA(cudaMemcpyAsync(Y.data(), b->evec, kMaxKry * kMaxKry * sizeof(double),
+                             cudaMemcpyDeviceToHost, c.st));
+    JCI_CUDA(cudaMemcpyAsync(&info, c.d_info, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+    JCI_CUDA(cudaStreamSynchronize(c.st));
+    JCI_CUDA(cudaGetLastError());
+    return info < 0 ? JCI_ERR_LINALG : JCI_OK;
+}
+
+// out = sum_i a[i] X_i + sum_i bb[i] Y_i with host coefficients
+static jci_status lincomb(Ctx &c, double *out, const double *X, const double *a, int mx,
+                          const double *Yv, const double *bb, int my) {
+    DavidsonBuffers *b = c.b;
+    std::vector<double> cc(2 * kMaxKry, 0.0);
+    for (int i = 0; i < mx; i++) cc[i] = a[i];
+    for (int i = 0; i < my; i++) cc[kMaxKry + i] = bb[i];
+    JCI_CUDA(cudaMemcpyAsync(b->coef, cc.data(), 2 * kMaxKry * sizeof(double),
+                             cudaMemcpyHostToDevice, c.st));
+    k_lincomb<<<grid_for(c.n), 256, 0, c.st>>>(out, c.n, c.ld, X, b->coef, mx, Yv,
+                                               b->coef + kMaxKry, my);
+    JCI_CUDA(cudaGetLastError());
+    return JCI_OK;
+}
+
+// V <- V Y^T[:, :k] (and C likewise): Ritz vectors of the first k roots
+static jci_status collapse(Ctx &c, int m, int k, const std::vector<double> &Y) {
+    DavidsonBuffers *b = c.b;
+    jci_status r;
+    for (int pass = 0; pass < 2; pass++) {
+        double *src = pass ? b->C : b->V;
+        for (int i = 0; i < k; i++)
+            if ((r = lincomb(c, b->X + i * c.ld, src, &Y[i * kMaxKry], m, nullptr, nullptr, 0)))
+                return r;
+        JCI_CUDA(cudaMemcpyAsync(src, b->X, (size_t)k * c.ld * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, c.st));
+        JCI_CUDA(cudaMemsetAsync(src + k * c.ld, 0, (size_t)(b->cap - k) * c.ld * sizeof(double),
+                                 c.st));
+    }
+    return JCI_OK;
+}
+
+// orthonormalise t against V_0..V_{m-1} (npass classical Gram-Schmidt
+// passes) and normalise; returns the norm before the final normalisation in
+// *nrm.  With prescale, t is first scaled to unit length, so *nrm is the
+// fraction of t that lies outside the current space.
+static jci_status orthonormalize(Ctx &c, double *t, int m, int npass, double *nrm,
+                                 bool prescale = false) {
+    DavidsonBuffers *b = c.b;
+    jci_status r;
+    if (prescale) {
+        if ((r = dots(c, t, 1, t, nullptr))) return r;
+        k_normalize<<<grid_for(c.n), 256, 0, c.st>>>(t, c.n, b->dots);
+    }
+    for (int p = 0; p < npass && m > 0; p++) {
+        if ((r = dots(c, b->V, m, t, nullptr))) return r;
+        k_orth_update<<<grid_for(c.n), 256, 0, c.st>>>(t, c.n, c.ld, b->V, b->dots, m);
+    }
+    if ((r = dots(c, t, 1, t, nullptr))) return r;
+    double h = 0.0;
+    JCI_CUDA(cudaMemcpyAsync(&h, b->dots, sizeof(double), cudaMemcpyDeviceToHost, c.st));
+    k_normalize<<<grid_for(c.n), 256, 0, c.st>>>(t, c.n, b->dots);
+    JCI_CUDA(cudaStreamSynchronize(c.st));
+    JCI_CUDA(cudaGetLastError());
+    *nrm = sqrt(h);
+    return JCI_OK;
+}
+
+// Host-side Slater-rule element between two determinants, for the
+// prediagonalisation guess (init_diag_H_subspace, pdavidson.c:3963, with
+// the generic hmatels of action_util.c:119).
+static double host_hmat(const jci_space *s, long long di, long long dj);
+
+static void host_symeig(int n, std::vector<double> a, std::vector<double> &w,
+                        std::vector<double> &z);
+
+static jci_status initial_vectors(Ctx &c, const jci_davidson_opts *o) {
+    jci_space *s = c.s;
+    int kmin = o->krymin;
+    long long n = c.n;
+    std::vector<double> v0((size_t)kmin * n, 0.0);
+    if (o->prediagr == 1) {
+        int dim = (int)std::min<long long>(o->refdim, n);
+        std::vector<double> h((size_t)dim * dim), w, z;
+        for (int i = 0; i < dim; i++)
+            for (int j = 0; j < dim; j++) h[i * dim + j] = host_hmat(s, i, j);
+        host_symeig(dim, h, w, z);
+        for (int i = 0; i < kmin && i < dim; i++)
+            for (int j = 0; j < dim; j++) v0[(size_t)i * n + j] = z[(size_t)i * dim + j];
+    } else if (o->prediagr == 2) {
+        for (int i = 0; i < kmin; i++) v0[(size_t)i * n + i] = 1.0;
+    } else {
+        if (o->init) {
+            memcpy(v0.data(), o->init, sizeof(double) * kmin * n);
+        } else {
+            jci_status r = jci_read_vectors("ci.restart", kmin, (int)n, v0.data());
+            if (r) return r;
+        }
+    }
+    for (int i = 0; i < kmin; i++)
+        JCI_CUDA(cudaMemcpyAsync(c.b->V + i * c.ld, &v0[(size_t)i * n], n * sizeof(double),
+                                 cudaMemcpyHostToDevice, c.st));
+    JCI_CUDA(cudaStreamSynchronize(c.st));
+    return JCI_OK;
+}
+
+static jci_status run_sequential(Ctx &c, const jci_davidson_opts *o, bool mixed,
+                                 std::vector<double> &w, std::vector<double> &Y, int &ckdim,
+                                 int &citer, int &converged, double &rnorm) {
+    DavidsonBuffers *b = c.b;
+    std::vector<double> G(kMaxKry * kMaxKry, 0.0), yc(kMaxKry), ycv(kMaxKry);
+    int kmin = o->krymin, kmax = o->krymax, nroots = o->nroots;
+    bool fp32 = mixed;
+    int croot = 1, cflag = 0;
+    ckdim = kmin;
+    citer = 1;
+    jci_status r;
+    while (citer < o->maxiter && croot <= nroots) {
+        if ((r = sigma_block(c, 0, ckdim, fp32))) return r;
+        if ((r = gram_rows(c, 0, ckdim, G))) return r;
+        if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
+        while (ckdim < kmax) {
+            double th = w[croot - 1];
+            for (int i = 0; i < ckdim; i++) {
+                yc[i] = Y[(croot - 1) * kMaxKry + i];
+                ycv[i] = -th * yc[i];
+            }
+            if ((r = lincomb(c, b->r, b->C, yc.data(), ckdim, b->V, ycv.data(), ckdim)))
+                return r;
+            double rn2 = 0.0;
+            if ((r = dots(c, b->r, 1, b->r, &rn2))) return r;
+            rnorm = sqrt(rn2);
+            if (o->printlvl > 0)
+                printf("  iter %4d  root %d  E = %18.12f  ||r|| = %.3e%s\n", citer, croot,
+                       th + c.s->nucrep + c.s->frzcore, rnorm, fp32 ? "  (fp32 sigma)" : "");
+            if (fp32 && rnorm < o->switch_tol) {
+                // switch: recompute every sigma vector in FP64
+                fp32 = false;
+                if ((r = sigma_block(c, 0, ckdim, false))) return r;
+                if ((r = gram_rows(c, 0, ckdim, G))) return r;
+                if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
+                continue;
+            }
+            cflag = rnorm < o->restol ? (croot < nroots ? 1 : 2) : 0;
+            if (cflag == 2) break;
+            if (cflag == 1) {
+                croot++;
+                break;
+            }
+            k_precond<<<grid_for(c.n), 256, 0, c.st>>>(b->r, c.d->hd, th, b->t, c.n);
+            double nn;
+            if ((r = orthonormalize(c, b->t, ckdim, 1, &nn))) return r;
+            JCI_CUDA(cudaMemcpyAsync(b->V + ckdim * c.ld, b->t, c.n * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, c.st));
+            if ((r = sigma_block(c, ckdim, 1, fp32))) return r;
+            ckdim++;
+            if ((r = gram_rows(c, ckdim - 1, ckdim, G))) return r;
+            if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
+            citer++;
+        }
+        if ((r = collapse(c, ckdim, kmin, Y))) return r;
+        ckdim = kmin;
+        if (cflag == 2) break;
+    }
+    converged = cflag == 2;
+    return JCI_OK;
+}
+
+static jci_status run_block(Ctx &c, const jci_davidson_opts *o, bool mixed,
+                            std::vector<double> &w, std::vector<double> &Y, int &ckdim,
+                            int &citer, int &converged, double &rnorm) {
+    DavidsonBuffers *b = c.b;
+    std::vector<double> G(kMaxKry * kMaxKry, 0.0), yc(kMaxKry), ycv(kMaxKry);
+    int kmin = o->krymin, kmax = o->krymax, nroots = o->nroots;
+    bool fp32 = mixed;
+    ckdim = kmin;
+    citer = 1;
+    jci_status r;
+    if ((r = sigma_block(c, 0, ckdim, fp32))) return r;
+    if ((r = gram_rows(c, 0, ckdim, G))) return r;
+    if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
+    converged = 0;
+    while (citer < o->maxiter) {
+        // residuals of all roots
+        std::vector<double> rn(nroots);
+        double rmax = 0.0;
+        for (int k = 0; k < nroots; k++) {
+            double th = w[k];
+            for (int i = 0; i < ckdim; i++) {
+                yc[i] = Y[k * kMaxKry + i];
+                ycv[i] = -th * yc[i];
+            }
+            if ((r = lincomb(c, b->r, b->C, yc.data(), ckdim, b->V, ycv.data(), ckdim))) return r;
+            double rn2 = 0.0;
+            if ((r = dots(c, b->r, 1, b->r, &rn2))) return r;
+            rn[k] = sqrt(rn2);
+            rmax = std::max(rmax, rn[k]);
+        }
+        rnorm = rmax;
+        if (o->printlvl > 0) {
+            printf("  iter %4d  dim %2d ", citer, ckdim);
+            for (int k = 0; k < nroots; k++)
+                printf(" E%d = %.12f (%.2e)", k + 1, w[k] + c.s->nucrep + c.s->frzcore, rn[k]);
+            printf("%s\n", fp32 ? "  fp32" : "");
+        }
+        if (fp32 && rmax < o->switch_tol) {
+            fp32 = false;
+            if ((r = sigma_block(c, 0, ckdim, false))) return r;
+            if ((r = gram_rows(c, 0, ckdim, G))) return r;
+            if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
+            continue;
+        }
+        if (rmax < o->restol) {
+            converged = 1;
+            break;
+        }
+        int nnew = 0;
+        for (int k = 0; k < nroots; k++) if (rn[k] >= o->restol) nnew++;
+        if (ckdim + nnew > kmax) {
+            int keep = std::max(kmin, nroots);
+            if ((r = collapse(c, ckdim, keep, Y))) return r;
+            ckdim = keep;
+            if ((r = gram_rows(c, 0, ckdim, G))) return r;
+            if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
+            continue;
+        }
+        int added = 0;
+        for (int k = 0; k < nroots; k++) {
+            if (rn[k] < o->restol) continue;
+            double th = w[k];
+            for (int i = 0; i < ckdim; i++) {
+                yc[i] = Y[k * kMaxKry + i];
+                ycv[i] = -th * yc[i];
+            }
+            if ((r = lincomb(c, b->r, b->C, yc.data(), ckdim, b->V, ycv.data(), ckdim))) return r;
+            k_precond<<<grid_for(c.n), 256, 0, c.st>>>(b->r, c.d->hd, th, b->t, c.n);
+            double nn;
+            if ((r = orthonormalize(c, b->t, ckdim + added, 2, &nn, true))) return r;
+            if (!(nn > 1e-8)) continue;  // correction (numerically) inside the space
+            JCI_CUDA(cudaMemcpyAsync(b->V + (ckdim + added) * c.ld, b->t, c.n * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, c.st));
+            added++;
+        }
+        if (added == 0) break;
+        if ((r = sigma_block(c, ckdim, added, fp32))) return r;
+        ckdim += added;
+        if ((r = gram_rows(c, ckdim - added, ckdim, G))) return r;
+        if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
+        citer += added;
+    }
+    if ((r = collapse(c, ckdim, std::max(kmin, nroots), Y))) return r;
+    ckdim = std::max(kmin, nroots);
+    return JCI_OK;
+}
+
+jci_status davidson(jci_space *s, const jci_davidson_opts *o, double *energies, double *civec,
+                    jci_davidson_stats *stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (!s->have_ints) return JCI_ERR_STATE;
+    if (o->krymin < o->nroots || o->krymax < o->krymin || o->krymax > kMaxKry ||
+        o->nroots < 1 || o->krymax > s->ndets || o->maxiter < 1)
+        return JCI_ERR_ARG;
+    Ctx c;
+    c.s = s;
+    c.d = s->dev;
+    c.st = c.d->stream;
+    c.n = s->ndets;
+    JCI_CUDA(cudaSetDevice(c.d->device));
+    bool mixed = o->precision == JCI_MIXED;
+    int maxnew = std::max(o->krymin, o->nroots);
+    jci_status r = ensure_buffers(c, o->krymax, mixed, maxnew);
+    if (r) return r;
+    JCI_CUDA(cudaMalloc(&c.d_info, sizeof(int)));
+    std::vector<double> w(kMaxKry, 0.0), Y(kMaxKry * kMaxKry, 0.0);
+    int ckdim = 0, citer = 0, conv = 0;
+    double rnorm = 0.0;
+    r = initial_vectors(c, o);
+    if (!r) {
+        if (o->block)
+            r = run_block(c, o, mixed, w, Y, ckdim, citer, conv, rnorm);
+        else
+            r = run_sequential(c, o, mixed, w, Y, ckdim, citer, conv, rnorm);
+    }
+    cudaFree(c.d_info);
+    if (r) return r;
+    double core = s->nucrep + s->frzcore;
+    for (int k = 0; k < o->nroots; k++) energies[k] = w[k] + core;
+    std::vector<double> host;
+    if (civec || o->write_files) {
+        host.resize((size_t)std::max(o->krymin, o->nroots) * c.n);
+        for (int k = 0; k < std::max(o->krymin, o->nroots); k++)
+            JCI_CUDA(cudaMemcpyAsync(&host[(size_t)k * c.n], c.b->V + k * c.ld,
+                                     c.n * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+        JCI_CUDA(cudaStreamSynchronize(c.st));
+        if (civec) memcpy(civec, host.data(), sizeof(double) * o->nroots * c.n);
+    }
+    if (o->write_files) {
+        // pdavidson.c:343-347
+        if ((r = jci_write_vectors("civec", o->nroots, (int)c.n, host.data()))) return r;
+        if (!conv) {
+            if ((r = jci_write_vectors("ci.restart", o->krymin, (int)c.n, host.data()))) return r;
+            std::vector<double> hv((size_t)o->nroots * c.n);
+            for (int k = 0; k < o->nroots; k++)
+                JCI_CUDA(cudaMemcpy(&hv[(size_t)k * c.n], c.b->C + k * c.ld,
+                                    c.n * sizeof(double), cudaMemcpyDeviceToHost));
+            if ((r = jci_write_vectors("hvvec", o->nroots, (int)c.n, hv.data()))) return r;
+        }
+    }
+    if (stats) {
+        stats->iterations = citer;
+        stats->sigma_calls = c.sigma_calls;
+        stats->sigma_vectors = c.sigma_vecs;
+        stats->sigma_seconds = c.sigma_ms * 1e-3;
+        stats->total_seconds =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        stats->converged = conv;
+        stats->rnorm = rnorm;
+        stats->fp32_sigma_vectors = c.fp32_vecs;
+    }
+    return conv ? JCI_OK : JCI_ERR_NOCONV;
+}
+
+// ---- host helpers --------------------------------------------------------
+
+static inline double h1(const jci_space *s, int i, int j) {
+    return s->m1[pair_index(i, j)];
+}
+static inline double h2(const jci_space *s, int i, int j, int k, int l) {
+    return s->m2[eri_index(pair_index(i, j), pair_index(k, l))];
+}
+
+static int phase(const int *o, int ne, int io, int fo) {
+    int lo = std::min(io, fo), hi = std::max(io, fo), c = 0;
+    for (int i = 0; i < ne; i++) c += (o[i] > lo && o[i] < hi);
+    return (c & 1) ? -1 : 1;
+}
+
+static double host_hmat(const jci_space *s, long long di, long long dj) {
+    int k, pi, qi, pj, qj;
+    det_strings(s, di, &k, &pi, &qi);
+    det_strings(s, dj, &k, &pj, &qj);
+    int na = s->sp[0].nelec, nb = s->sp[1].nelec;
+    const int *ai = &s->sp[0].istr[(size_t)pi * na], *aj = &s->sp[0].istr[(size_t)pj * na];
+    const int *bi = &s->sp[1].istr[(size_t)qi * nb], *bj = &s->sp[1].istr[(size_t)qj * nb];
+    auto diff = [](const int *x, const int *y, int n, int *out) {
+        int c = 0;
+        for (int i = 0; i < n; i++) {
+            bool f = false;
+            for (int j = 0; j < n; j++) f |= (x[i] == y[j]);
+            if (!f) out[c++] = x[i];
+        }
+        return c;
+    };
+    int ax[kMaxElec], af[kMaxElec], bx[kMaxElec], bf[kMaxElec];
+    int nax = diff(ai, aj, na, ax), nbx = diff(bi, bj, nb, bx);
+    diff(aj, ai, na, af);
+    diff(bj, bi, nb, bf);
+    if (nax + nbx > 2) return 0.0;
+    auto one = [&](const int *o1, int n1, int io, int fo, const int *o2, int n2) {
+        double v = h1(s, io, fo);
+        for (int i = 0; i < n1; i++)
+            if (o1[i] != io) v += h2(s, o1[i], o1[i], io, fo) - h2(s, o1[i], io, o1[i], fo);
+        for (int i = 0; i < n2; i++) v += h2(s, o2[i], o2[i], io, fo);
+        return phase(o1, n1, io, fo) * v;
+    };
+    if (nax + nbx == 0) {
+        double v = 0.0;
+        for (int i = 0; i < na; i++) {
+            v += h1(s, ai[i], ai[i]);
+            for (int j = 0; j < i; j++)
+                v += h2(s, ai[i], ai[i], ai[j], ai[j]) - h2(s, ai[i], ai[j], ai[i], ai[j]);
+        }
+        for (int i = 0; i < nb; i++) {
+            v += h1(s, bi[i], bi[i]);
+            for (int j = 0; j < i; j++)
+                v += h2(s, bi[i], bi[i], bi[j], bi[j]) - h2(s, bi[i], bi[j], bi[i], bi[j]);
+        }
+        for (int i = 0; i < na; i++)
+            for (int j = 0; j < nb; j++) v += h2(s, ai[i], ai[i], bi[j], bi[j]);
+        return v;
+    }
+    if (nax == 1 && nbx == 0) return one(ai, na, ax[0], af[0], bi, nb);
+    if (nax == 0 && nbx == 1) return one(bi, nb, bx[0], bf[0], ai, na);
+    if (nax == 1 && nbx == 1)
+        return phase(ai, na, ax[0], af[0]) * phase(bi, nb, bx[0], bf[0]) *
+               h2(s, ax[0], af[0], bx[0], bf[0]);
+    const int *o = nax == 2 ? ai : bi;
+    int n = nax == 2 ? na : nb;
+    int *x = nax == 2 ? ax : bx, *f = nax == 2 ? af : bf;
+    // io = (higher, lower), fo ascending; phase of the first replacement in
+    // the string times that of the second in the intermediate string
+    int t1[kMaxElec], m = 0;
+    for (int i = 0; i < n; i++)
+        if (o[i] != x[1]) t1[m++] = o[i];
+    int kk = m;
+    while (kk > 0 && t1[kk - 1] > f[0]) {
+        t1[kk] = t1[kk - 1];
+        kk--;
+    }
+    t1[kk] = f[0];
+    int p = phase(o, n, x[1], f[0]) * phase(t1, n, x[0], f[1]);
+    return p * (h2(s, x[1], f[0], x[0], f[1]) - h2(s, x[1], f[1], x[0], f[0]));
+}
+
+static void host_symeig(int n, std::vector<double> a, std::vector<double> &w,
+                        std::vector<double> &z) {
+    std::vector<double> v((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++) v[(size_t)i * n + i] = 1.0;
+    for (int sweep = 0; sweep < 100; sweep++) {
+        double off = 0.0;
+        for (int p = 0; p < n; p++)
+            for (int q = p + 1; q < n; q++) off += a[p * n + q] * a[p * n + q];
+        if (off < 1e-30) break;
+        for (int p = 0; p < n; p++)
+            for (int q = p + 1; q < n; q++) {
+                double apq = a[p * n + q];
+                if (fabs(apq) < 1e-300) continue;
+                double th = (a[q * n + q] - a[p * n + p]) / (2 * apq);
+                double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+                double cc = 1.0 / sqrt(t * t + 1.0), ss = t * cc;
+                for (int k = 0; k < n; k++) {
+                    double akp = a[k * n + p], akq = a[k * n + q];
+                    a[k * n + p] = cc * akp - ss * akq;
+                    a[k * n + q] = ss * akp + cc * akq;
+                }
+                for (int k = 0; k < n; k++) {
+                    double apk = a[p * n + k], aqk = a[q * n + k];
+                    a[p * n + k] = cc * apk - ss * aqk;
+                    a[q * n + k] = ss * apk + cc * aqk;
+                }
+                for (int k = 0; k < n; k++) {
+                    double vkp = v[k * n + p], vkq = v[k * n + q];
+                    v[k * n + p] = cc * vkp - ss * vkq;
+                    v[k * n + q] = ss * vkp + cc * vkq;
+                }
+            }
+    }
+    std::vector<int> ord(n);
+    for (int i = 0; i < n; i++) ord[i] = i;
+    std::stable_sort(ord.begin(), ord.end(),
+                     [&](int x, int y) { return a[x * n + x] < a[y * n + y]; });
+    w.assign(n, 0.0);
+    z.assign((size_t)n * n, 0.0);
+    for (int k = 0; k < n; k++) {
+        w[k] = a[ord[k] * n + ord[k]];
+        for (int i = 0; i < n; i++) z[(size_t)k * n + i] = v[(size_t)i * n + ord[k]];
+    }
+}
+
+}  // namespace jci

@@ -1,0 +1,416 @@
+// jci_fci.cu -- sigma = H c for spaces with one electron-occupation group
+// per spin (FCI, CAS, and DOCC+ACTV with xlevel 0).
+//
+// With one group every alpha string pairs with every beta string, so the
+// CI vector is an Nalpha x Nbeta row-major matrix (det = p * Nbeta + q,
+// pdavidson.c:4757 with a single (p,q) pair), every string has the same
+// number of singles / doubles, and the excitation tables can be stored
+// transposed ([excitation][string]) so that the threads of a CTA, which own
+// consecutive beta strings, read them coalesced.
+//
+// Kernel layout: one CTA per alpha string Ia computes the whole row
+// sigma(Ia, :) in registers (each thread owns Nbeta / blockDim columns):
+//   1. the CTA's own row c(Ia, :) is staged in shared memory; beta singles
+//      and beta doubles gather from it (hmatels_1x / hmatels_2xaa on the
+//      beta string, action_util.c:210,237);
+//   2. alpha singles Ja are processed R rows at a time: rows c(Ja, :) and
+//      the integral rows phase_a * (pa|.) are staged in shared memory; each
+//      column applies the alpha single (same beta string, hmatels_1x) and
+//      every beta single of its string against each staged row
+//      (hmatels_2xab, action_util.c:250), so one load of a beta excitation
+//      entry serves R rows;
+//   3. alpha doubles stream rows c(Ja, :) straight from global memory
+//      (coalesced, L2-resident for the sizes that fit).
+// Each sigma element is written once (gather form): no atomics, and the
+// result is bitwise reproducible run to run.
+#include <algorithm>
+#include <cstdio>
+#include <vector>
+
+#include "jci_kernels.cuh"
+
+namespace jci {
+
+template <typename T>
+struct FciSpin {
+    T *a1T = nullptr;     // [single][string] one-body part, no phase
+    T *joccT = nullptr;   // [pair][string] sum_{m in string} (mm|pair)
+    T *dblH = nullptr;    // [double][string] value with phase
+};
+
+struct FciTables {
+    int na = 0, nb = 0, sa = 0, sb = 0, da = 0, db = 0, npair = 0;
+    int *dblJ[2] = {nullptr, nullptr};   // [double][string] target string
+    FciSpin<double> d[2];
+    FciSpin<float> f[2];
+    size_t smem_max = 0;
+    int tuned_nt[2] = {0, 0}, tuned_R[2] = {0, 0};  // per precision (autotuned)
+    float tuned_ms[2] = {0.f, 0.f};
+};
+
+bool fci_supported(const jci_space *s) {
+    const DeviceState *d = s->dev;
+    if (!d || !d->single_group || !d->fci) return false;
+    return d->fci->smem_max > 0;
+}
+
+void fci_free(DeviceState *d) {
+    FciTables *f = d->fci;
+    if (!f) return;
+    for (int s = 0; s < 2; s++) {
+        cudaFree(f->dblJ[s]);
+        cudaFree(f->d[s].a1T); cudaFree(f->d[s].joccT); cudaFree(f->d[s].dblH);
+        cudaFree(f->f[s].a1T); cudaFree(f->f[s].joccT); cudaFree(f->f[s].dblH);
+    }
+    delete f;
+    d->fci = nullptr;
+}
+
+// ---- table construction -----------------------------------------------
+
+__global__ void k_fci_tables(int nstr, int nelec, int ns, int nd, int npair,
+                             const int *__restrict__ istr, const uint2 *__restrict__ doub,
+                             const double *__restrict__ a1, const double *__restrict__ m2,
+                             double *a1T, float *a1Tf, double *joccT, float *joccTf,
+                             int *dblJ, double *dblH, float *dblHf) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nstr) return;
+    for (int e = 0; e < ns; e++) {
+        double v = a1[(long long)s * ns + e];
+        a1T[(long long)e * nstr + s] = v;
+        a1Tf[(long long)e * nstr + s] = (float)v;
+    }
+    const int *o = istr + (long long)s * nelec;
+    for (int p = 0; p < npair; p++) {
+        double v = 0.0;
+        for (int k = 0; k < nelec; k++) v += m2[eri_index(pair_index(o[k], o[k]), p)];
+        joccT[(long long)p * nstr + s] = v;
+        joccTf[(long long)p * nstr + s] = (float)v;
+    }
+    for (int e = 0; e < nd; e++) {
+        uint2 x = doub[(long long)s * nd + e];
+        int i0 = x.y & 0xff, f0 = (x.y >> 8) & 0xff, i1 = (x.y >> 16) & 0xff, f1 = x.y >> 24;
+        double h = m2[eri_index(pair_index(i0, f0), pair_index(i1, f1))] -
+                   m2[eri_index(pair_index(i0, f1), pair_index(i1, f0))];
+        if (x.x >> 31) h = -h;
+        dblJ[(long long)e * nstr + s] = (int)(x.x & 0x3fffffffu);
+        dblH[(long long)e * nstr + s] = h;
+        dblHf[(long long)e * nstr + s] = (float)h;
+    }
+}
+
+template <typename T>
+struct FciArgs {
+    int na, nb, sa, sb, da, db, npair, R;
+    const uint32_t *fsA, *fsB;    // [single][string] target | sign << 31
+    const uint16_t *fpA, *fpB;    // [single][string] pair index
+    const T *a1A, *a1B;           // [single][string]
+    const T *jA, *jB;             // [pair][string]
+    const int *dJA, *dJB;         // [double][string]
+    const T *dHA, *dHB;
+    const T *hd;                  // <i|H|i>
+    const T *m2;                  // packed (pq|rs)
+};
+
+template <typename T>
+__device__ __forceinline__ T flip(T w, uint32_t neg) {
+    return neg ? -w : w;
+}
+
+template <typename T, int ITEMS>
+__global__ void __launch_bounds__(ITEMS <= 2 ? 1024 : 512)
+    k_sigma_fci(FciArgs<T> a, const T *__restrict__ V, T *__restrict__ S) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *rows = reinterpret_cast<T *>(smem_raw);         // (1 + R) x nb
+    T *vrow = rows + (size_t)(1 + a.R) * a.nb;         // R x npair
+    T *jrow = vrow + (size_t)a.R * a.npair;            // npair
+    T *coef = jrow + a.npair;                          // R
+    int *pas = reinterpret_cast<int *>(coef + a.R);    // R pair of alpha single
+    uint32_t *sgn = reinterpret_cast<uint32_t *>(pas + a.R);  // R
+    const int nb = a.nb, tid = threadIdx.x, nt = blockDim.x;
+    const int Ia = blockIdx.x;
+    const T *crow = V + (long long)Ia * nb;
+    for (int i = tid; i < nb; i += nt) rows[i] = crow[i];
+    for (int p = tid; p < a.npair; p += nt) jrow[p] = a.jA[(long long)p * a.na + Ia];
+    __syncthreads();
+
+    T acc[ITEMS];
+#pragma unroll
+    for (int it = 0; it < ITEMS; it++) {
+        int Ib = tid + it * nt;
+        acc[it] = T(0);
+        if (Ib >= nb) continue;
+        T x = a.hd[(long long)Ia * nb + Ib] * rows[Ib];
+        // beta singles within the row (hmatels_1x with alpha as the other string)
+        for (int f = 0; f < a.sb; f++) {
+            long long o = (long long)f * nb + Ib;
+            uint32_t e = a.fsB[o];
+            T h = a.a1B[o] + jrow[a.fpB[o]];
+            x += flip(h, e >> 31) * rows[e & 0x3fffffffu];
+        }
+        // beta doubles within the row
+        for (int f = 0; f < a.db; f++) {
+            long long o = (long long)f * nb + Ib;
+            x += a.dHB[o] * rows[a.dJB[o]];
+        }
+        acc[it] = x;
+    }
+
+    // alpha singles (with alpha x beta doubles), R staged rows at a time
+    for (int e0 = 0; e0 < a.sa; e0 += a.R) {
+        const int nr = min(a.R, a.sa - e0);
+        __syncthreads();
+        if (tid < nr) {
+            long long o = (long long)(e0 + tid) * a.na + Ia;
+            uint32_t e = a.fsA[o];
+            sgn[tid] = e >> 31;
+            pas[tid] = a.fpA[o];
+            coef[tid] = flip(a.a1A[o], e >> 31);
+        }
+        __syncthreads();
+        for (int r = 0; r < nr; r++) {
+            long long o = (long long)(e0 + r) * a.na + Ia;
+            int Ja = (int)(a.fsA[o] & 0x3fffffffu);
+            const T *src = V + (long long)Ja * nb;
+            T *dst = rows + (size_t)(1 + r) * nb;
+            for (int i = tid; i < nb; i += nt) dst[i] = src[i];
+            int pa = pas[r];
+            uint32_t sg = sgn[r];
+            for (int p = tid; p < a.npair; p += nt)
+                vrow[(size_t)r * a.npair + p] = flip(a.m2[eri_index(pa, p)], sg);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int it = 0; it < ITEMS; it++) {
+            int Ib = tid + it * nt;
+            if (Ib >= nb) continue;
+            T x = acc[it];
+#pragma unroll 4
+            for (int r = 0; r < nr; r++) {
+                T h = coef[r] + flip(a.jB[(long long)pas[r] * nb + Ib], sgn[r]);
+                x += h * rows[(size_t)(1 + r) * nb + Ib];
+            }
+            for (int f = 0; f < a.sb; f++) {
+                long long o = (long long)f * nb + Ib;
+                uint32_t e = a.fsB[o];
+                int J = (int)(e & 0x3fffffffu), pr = a.fpB[o];
+                uint32_t neg = e >> 31;
+                const T *rr = rows + nb + J;
+                const T *vv = vrow + pr;
+#pragma unroll 4
+                for (int r = 0; r < nr; r++)
+                    x += flip(vv[(size_t)r * a.npair], neg) * rr[(size_t)r * nb];
+            }
+            acc[it] = x;
+        }
+    }
+
+    // alpha doubles: rows streamed from global memory
+    for (int f = 0; f < a.da; f++) {
+        long long o = (long long)f * a.na + Ia;
+        int Ja = a.dJA[o];
+        T h = a.dHA[o];
+        const T *src = V + (long long)Ja * nb;
+#pragma unroll
+        for (int it = 0; it < ITEMS; it++) {
+            int Ib = tid + it * nt;
+            if (Ib < nb) acc[it] += h * src[Ib];
+        }
+    }
+    T *dst = S + (long long)Ia * nb;
+#pragma unroll
+    for (int it = 0; it < ITEMS; it++) {
+        int Ib = tid + it * nt;
+        if (Ib < nb) dst[Ib] = acc[it];
+    }
+}
+
+static size_t fci_smem(int nb, int npair, int R, size_t w) {
+    return (size_t)(1 + R) * nb * w + (size_t)R * npair * w + (size_t)npair * w +
+           (size_t)R * (w + 8) + 64;
+}
+
+template <typename T, int ITEMS>
+static jci_status set_smem_attr(size_t bytes) {
+    JCI_CUDA(cudaFuncSetAttribute(k_sigma_fci<T, ITEMS>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return JCI_OK;
+}
+
+jci_status fci_prepare(jci_space *s) {
+    DeviceState *d = s->dev;
+    if (!d->single_group) return JCI_OK;
+    const SpinSpace &A = s->sp[0], &B = s->sp[1];
+    if (A.nstr >= (1 << 30) || B.nstr >= (1 << 30) || d->npair > 65535) return JCI_OK;
+    if (B.nstr > 32 * 512) return JCI_OK;  // register-resident row limit
+    cudaStream_t st = d->stream;
+    FciTables *f = d->fci;
+    if (!f) {
+        f = new FciTables();
+        d->fci = f;
+        f->na = A.nstr; f->nb = B.nstr;
+        f->sa = A.max_sing; f->sb = B.max_sing;
+        f->da = A.max_doub; f->db = B.max_doub;
+        f->npair = d->npair;
+        for (int sp = 0; sp < 2; sp++) {
+            const SpinSpace &X = s->sp[sp];
+            size_t n = (size_t)X.nstr;
+            size_t ns = (size_t)X.max_sing * n + 1, nd = (size_t)X.max_doub * n + 1;
+            size_t npn = (size_t)d->npair * n;
+            JCI_CUDA(cudaMalloc(&f->dblJ[sp], nd * sizeof(int)));
+            JCI_CUDA(cudaMalloc(&f->d[sp].a1T, ns * sizeof(double)));
+            JCI_CUDA(cudaMalloc(&f->d[sp].joccT, npn * sizeof(double)));
+            JCI_CUDA(cudaMalloc(&f->d[sp].dblH, nd * sizeof(double)));
+            JCI_CUDA(cudaMalloc(&f->f[sp].a1T, ns * sizeof(float)));
+            JCI_CUDA(cudaMalloc(&f->f[sp].joccT, npn * sizeof(float)));
+            JCI_CUDA(cudaMalloc(&f->f[sp].dblH, nd * sizeof(float)));
+        }
+        int dev = d->device, optin = 0;
+        JCI_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        f->smem_max = (size_t)optin;
+        // the kernel needs at least the own row plus one staged row
+        if (fci_smem(f->nb, f->npair, 1, sizeof(double)) > f->smem_max) f->smem_max = 0;
+    }
+    for (int sp = 0; sp < 2; sp++) {
+        const SpinTables &t = d->t[sp];
+        const SpinSpace &X = s->sp[sp];
+        k_fci_tables<<<(X.nstr + 127) / 128, 128, 0, st>>>(
+            X.nstr, X.nelec, X.max_sing, X.max_doub, d->npair, t.istr, t.doub, t.a1, d->m2,
+            f->d[sp].a1T, f->f[sp].a1T, f->d[sp].joccT, f->f[sp].joccT, f->dblJ[sp],
+            f->d[sp].dblH, f->f[sp].dblH);
+    }
+    JCI_CUDA(cudaGetLastError());
+    return JCI_OK;
+}
+
+template <typename T>
+static jci_status launch_one(const FciArgs<T> &a, int nt, size_t smem, int na, const T *v, T *o,
+                             cudaStream_t st) {
+    int items = (a.nb + nt - 1) / nt;
+    jci_status r = JCI_OK;
+    dim3 grid(na);
+#define JCI_LAUNCH(IT)                                                          \
+    do {                                                                        \
+        if ((r = set_smem_attr<T, IT>(smem)) != JCI_OK) return r;              \
+        k_sigma_fci<T, IT><<<grid, nt, smem, st>>>(a, v, o);                    \
+    } while (0)
+    if (items <= 2) JCI_LAUNCH(2);
+    else if (items <= 4) JCI_LAUNCH(4);
+    else if (items <= 8) JCI_LAUNCH(8);
+    else if (items <= 16) JCI_LAUNCH(16);
+    else JCI_LAUNCH(32);
+#undef JCI_LAUNCH
+    return JCI_OK;
+}
+
+// Pick (threads per CTA, staged rows per pass) for this space by timing the
+// admissible candidates on scratch vectors; cached per precision.
+template <typename T>
+static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
+    DeviceState *d = s->dev;
+    FciTables *f = d->fci;
+    const int prec = sizeof(T) == 8 ? 0 : 1;
+    size_t w = sizeof(T);
+    long long n = (long long)f->na * f->nb;
+    T *v = nullptr, *o = nullptr;
+    JCI_CUDA(cudaMalloc(&v, n * w));
+    JCI_CUDA(cudaMalloc(&o, n * w));
+    JCI_CUDA(cudaMemsetAsync(v, 0, n * w, st));
+    float best = 1e30f;
+    int bnt = 0, bR = 0;
+    const int nts[] = {128, 256, 512, 1024};
+    const int Rs[] = {1, 2, 4, 8, 16};
+    cudaEvent_t e0, e1;
+    JCI_CUDA(cudaEventCreate(&e0));
+    JCI_CUDA(cudaEventCreate(&e1));
+    for (int nt : nts) {
+        int items = (f->nb + nt - 1) / nt;
+        if (items > 32 || (nt == 1024 && items > 2)) continue;
+        if (nt > 32 * ((f->nb + 31) / 32) && nt > 128) continue;  // idle threads
+        for (int R : Rs) {
+            if (R > f->sa && R > 1) continue;
+            size_t smem = fci_smem(f->nb, f->npair, R, w);
+            if (smem > f->smem_max) continue;
+            a.R = R;
+            jci_status r = launch_one<T>(a, nt, smem, f->na, v, o, st);
+            if (r) return r;
+            JCI_CUDA(cudaEventRecord(e0, st));
+            for (int k = 0; k < 2; k++)
+                if ((r = launch_one<T>(a, nt, smem, f->na, v, o, st))) return r;
+            JCI_CUDA(cudaEventRecord(e1, st));
+            JCI_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            JCI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) {
+                best = ms;
+                bnt = nt;
+                bR = R;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(v);
+    cudaFree(o);
+    if (!bnt) return JCI_ERR_SPACE;
+    f->tuned_nt[prec] = bnt;
+    f->tuned_R[prec] = bR;
+    f->tuned_ms[prec] = best / 2;
+    return JCI_OK;
+}
+
+void fci_tuning(const jci_space *s, int precision, int *nt, int *R, float *ms) {
+    const FciTables *f = s->dev ? s->dev->fci : nullptr;
+    int p = precision == JCI_FP32 ? 1 : 0;
+    *nt = f ? f->tuned_nt[p] : 0;
+    *R = f ? f->tuned_R[p] : 0;
+    *ms = f ? f->tuned_ms[p] : 0.f;
+}
+
+template <typename T>
+static jci_status launch_fci(jci_space *s, int nvec, const T *V, T *S, long long ld,
+                             cudaStream_t st) {
+    DeviceState *d = s->dev;
+    FciTables *f = d->fci;
+    const int prec = sizeof(T) == 8 ? 0 : 1;
+    FciArgs<T> a;
+    a.na = f->na; a.nb = f->nb; a.sa = f->sa; a.sb = f->sb; a.da = f->da; a.db = f->db;
+    a.npair = f->npair;
+    a.fsA = d->t[0].fsing; a.fsB = d->t[1].fsing;
+    a.fpA = d->t[0].fspair; a.fpB = d->t[1].fspair;
+    a.dJA = f->dblJ[0]; a.dJB = f->dblJ[1];
+    if (prec == 0) {
+        a.a1A = (const T *)f->d[0].a1T; a.a1B = (const T *)f->d[1].a1T;
+        a.jA = (const T *)f->d[0].joccT; a.jB = (const T *)f->d[1].joccT;
+        a.dHA = (const T *)f->d[0].dblH; a.dHB = (const T *)f->d[1].dblH;
+        a.hd = (const T *)d->hd; a.m2 = (const T *)d->m2;
+    } else {
+        a.a1A = (const T *)f->f[0].a1T; a.a1B = (const T *)f->f[1].a1T;
+        a.jA = (const T *)f->f[0].joccT; a.jB = (const T *)f->f[1].joccT;
+        a.dHA = (const T *)f->f[0].dblH; a.dHB = (const T *)f->f[1].dblH;
+        a.hd = (const T *)d->hdf; a.m2 = (const T *)d->m2f;
+    }
+    size_t w = sizeof(T);
+    int &nt = f->tuned_nt[prec], &R = f->tuned_R[prec];
+    if (nt == 0) {
+        jci_status r = autotune<T>(s, a, st);
+        if (r) return r;
+    }
+    a.R = R;
+    for (int c = 0; c < nvec; c++) {
+        jci_status r = launch_one<T>(a, nt, fci_smem(f->nb, f->npair, R, w), f->na,
+                                     V + c * ld, S + c * ld, st);
+        if (r) return r;
+    }
+    JCI_CUDA(cudaGetLastError());
+    return JCI_OK;
+}
+
+jci_status fci_sigma(jci_space *s, int nvec, const void *v, void *sig, long long ld,
+                     int precision, cudaStream_t st) {
+    if (precision == JCI_FP32)
+        return launch_fci<float>(s, nvec, (const float *)v, (float *)sig, ld, st);
+    return launch_fci<double>(s, nvec, (const double *)v, (double *)sig, ld, st);
+}
+
+}  // namespace jci

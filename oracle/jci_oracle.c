@@ -555,11 +555,18 @@ double jo_hmatel(const jo_space *s, const double *m1, const double *m2,
 void jo_sigma(const jo_space *s, const double *m1, const double *m2,
               int nvec, const double *V, double *S)
 {
+        jo_sigma_range(s, m1, m2, nvec, V, S, 0, s->ndets);
+}
+
+void jo_sigma_range(const jo_space *s, const double *m1, const double *m2,
+                    int nvec, const double *V, double *S, long long d0,
+                    long long d1)
+{
         const struct jo_spin *A = &s->sp[0], *B = &s->sp[1];
         int na = A->nelec, nb = B->nelec;
         long long N = s->ndets;
         double *acc = malloc(sizeof(double) * nvec);
-        for (long long d = 0; d < N; d++) {
+        for (long long d = d0; d < d1 && d < N; d++) {
                 int k, p, q;
                 det_strings(s, d, &k, &p, &q);
                 const int *sa = A->istr + (long long)p * na;

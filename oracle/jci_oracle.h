@@ -50,6 +50,10 @@ double jo_hmatel(const jo_space *s, const double *m1, const double *m2,
 /* S = H V for nvec vectors stored vector-major (full-row gather). */
 void jo_sigma(const jo_space *s, const double *m1, const double *m2,
               int nvec, const double *V, double *S);
+/* Rows d0 <= d < d1 of the same (S holds all ndets per vector). */
+void jo_sigma_range(const jo_space *s, const double *m1, const double *m2,
+                    int nvec, const double *V, double *S, long long d0,
+                    long long d1);
 
 /* Root-sequential Davidson (pdavidson.c:39).  Returns iterations taken
  * (>= 0) or a negative error.  energies[nroots] include totcore; civec is

@@ -242,6 +242,57 @@ void ref_sigma(double *m1, double *m2, int nvec, const double *V, double *C)
         shim_ga_reset();
 }
 
+/* Bounded samples of the reference's sigma for CPU timing: ref_sigma_prepare
+ * sets up V, C, D and W once; ref_sigma_rows_timed runs the reference's
+ * row-range kernel compute_cblock_Hfastest (pdavidson.c:1296) for rows
+ * [row0, row0 + nrows) of the upper triangle and returns its wall time in
+ * seconds (setup excluded).  The partial C it accumulates is not a sigma. */
+#include <time.h>
+static int T_v, T_c, T_d, T_w, T_nvec;
+static double *T_m1, *T_m2;
+
+int ref_sigma_prepare(double *m1, double *m2, int nvec, const double *V)
+{
+        shim_ga_reset();
+        int vd[2] = {nvec, S.ndets}, vc[2] = {nvec, -1};
+        T_v = NGA_Create(C_DBL, 2, vd, "V", vc);
+        T_c = NGA_Duplicate(T_v, "C");
+        int nd[1] = {S.ndets}, nc[1] = {-1};
+        T_d = NGA_Create(C_DBL, 1, nd, "D", nc);
+        T_w = make_wlist();
+        T_nvec = nvec;
+        T_m1 = m1;
+        T_m2 = m2;
+        memcpy(shim_ga_data(T_v), V, sizeof(double) * nvec * S.ndets);
+        return 0;
+}
+
+double ref_sigma_rows_timed(int row0, int nrows)
+{
+        int ccols = T_nvec, crows = nrows;
+        double *cdata = calloc((size_t)ccols * crows, sizeof(double));
+        int **wi = NULL;
+        int *widata = allocate_mem_int_cont(&wi, 3, crows);
+        int lo[2] = {row0, 0}, hi[2] = {row0 + nrows - 1, 2}, ld[1] = {3};
+        NGA_Get(T_w, lo, hi, widata, ld);
+        int *cindx = malloc(sizeof(int) * ccols);
+        for (int i = 0; i < ccols; i++) cindx[i] = i;
+        struct timespec a, b;
+        clock_gettime(CLOCK_MONOTONIC, &a);
+        compute_cblock_Hfastest(cdata, ccols, crows, wi, T_w, T_v, T_d, 0, S.pstr,
+                                S.peosp, S.pegrps, S.qstr, S.qeosp, S.qegrps, S.pq,
+                                S.num_pq, T_m1, T_m2, S.ci_aelec, S.ci_belec,
+                                S.intorb, S.ndets, S.ci_orbs, S.ndocc, S.nactv,
+                                T_c, row0, row0 + nrows - 1, cindx);
+        clock_gettime(CLOCK_MONOTONIC, &b);
+        free(cindx);
+        free(cdata);
+        deallocate_mem_cont_int(&wi, widata);
+        return (b.tv_sec - a.tv_sec) + 1e-9 * (b.tv_nsec - a.tv_nsec);
+}
+
+void ref_sigma_release(void) { shim_ga_reset(); }
+
 /* Full reference Davidson solve (pdavidson, pdavidson.c:39) run in
  * directory `workdir` (it writes civec / ci.restart / hvvec there).  On
  * return civec_out holds the nroots result vectors (vector-major) read back

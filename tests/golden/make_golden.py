@@ -1,0 +1,106 @@
+"""Generate the golden fixtures in this directory from the reference itself.
+
+Runs the reference's own mpi_source C code (oracle/_ref/libjayci_ref.so,
+built from the read-only reference tree by ``make -C oracle``) single-rank
+and single-threaded on seeded synthetic integrals, and stores what it
+produces: string lists, group tables, (p,q) pairs, determinant triples,
+yij/cij tables, excitation lists, <i|H|i>, sigma on seeded random vectors
+and Davidson energies / vectors.
+
+    OMP_NUM_THREADS=1 python tests/golden/make_golden.py
+
+Only this script touches the reference; the tests read the .npz files.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from jayci_b200.synth import make_integrals  # noqa: E402
+from oracle.oracle import RefSpace  # noqa: E402
+
+# name: (&general values, integral rank, seed, davidson options or None)
+CASES = {
+    # CAS(6,6): 3 alpha / 3 beta electrons in 6 orbitals, 400 determinants
+    "cas6_6": (dict(electrons=6, orbitals=6), 6, 11,
+               dict(krymin=4, krymax=10, nroots=2, refdim=8)),
+    # odd electron count: 4 alpha / 3 beta in 7 orbitals
+    "cas7_7": (dict(electrons=7, orbitals=7), 7, 12,
+               dict(krymin=3, krymax=8, nroots=1, refdim=6)),
+    # truncated: 2 DOCC, 4 ACTV, 2 VIRT, excitation level 2
+    "trunc6_8_x2": (dict(electrons=6, orbitals=8, ndocc=2, nactv=4, xlvl=2), 8, 13,
+                    dict(krymin=4, krymax=10, nroots=2, refdim=8)),
+    # truncated with a frozen core and a frozen virtual, excitation level 1
+    "trunc10_12_fc_x1": (dict(electrons=10, orbitals=12, nfrzc=1, ndocc=3, nactv=4,
+                              nfrzv=1, xlvl=1), 10, 14,
+                         dict(krymin=3, krymax=8, nroots=1, refdim=6)),
+    # the 63 504-determinant CAS(10,10) workload (seed 101, rank 10)
+    "cas10_10": (dict(electrons=10, orbitals=10), 10, 101,
+                 dict(krymin=4, krymax=12, nroots=1, refdim=8)),
+}
+
+
+def make(name):
+    gen, rank, seed, dav = CASES[name]
+    ref = RefSpace(gen["electrons"], gen["orbitals"], gen.get("nfrzc", 0),
+                   gen.get("ndocc", 0), gen.get("nactv"), gen.get("nfrzv", 0),
+                   gen.get("xlvl", 0))
+    ints = make_integrals(ref.norb, rank, seed)
+    m1, m2 = ints.packed()
+    out = dict(general=np.array([gen["electrons"], gen["orbitals"], gen.get("nfrzc", 0),
+                                 gen.get("ndocc", 0), ref.nactv, gen.get("nfrzv", 0),
+                                 gen.get("xlvl", 0)]),
+               rank=rank, seed=seed, m1=m1, m2=m2, e_nuc=ints.e_nuc,
+               sizes=np.array([ref.na, ref.nb, ref.norb, ref.nastr, ref.nbstr, ref.pegrps,
+                               ref.qegrps, ref.npq, ref.ndets]))
+    for sp in (0, 1):
+        istr, b1, vx, nv = ref.strings(sp)
+        out[f"istr{sp}"] = istr
+        out[f"byte1_{sp}"] = b1
+        out[f"eosp{sp}"] = ref.eospaces(sp)[:, :6]
+        if ref.ndets < 100000:
+            y, c = ref.yij_cij(sp)
+            out[f"yij{sp}"] = y
+            out[f"cij{sp}"] = c
+        # excitation lists of a few strings into every group
+        ns = ref.nastr if sp == 0 else ref.nbstr
+        ng = ref.pegrps if sp == 0 else ref.qegrps
+        rows = []
+        for s in sorted(set([0, 1, ns // 3, ns // 2, ns - 1])):
+            for g in range(ng):
+                for nrep in (1, 2):
+                    for r in ref.excitations(sp, nrep, s, g):
+                        rows.append([s, g, nrep] + list(r))
+        out[f"exc{sp}"] = np.array(rows, np.int32).reshape(-1, 9)
+    out["pq"] = ref.pq()
+    out["wlist"] = ref.wlist()
+    out["hdiag"] = ref.hdiag(m1, m2)
+    rng = np.random.default_rng(seed + 1000)
+    V = rng.standard_normal((2, ref.ndets))
+    out["sigma_v"] = V
+    out["sigma"] = ref.sigma(m1, m2, V)
+    if dav:
+        civ, _ = ref.davidson(m1, m2, ints.e_nuc, 0.0, maxiter=500, prediagr=1,
+                              restol=1e-9, **dav)
+        H = None
+        # Rayleigh quotients of the reference's result vectors (its energies)
+        S = ref.sigma(m1, m2, civ)
+        e = np.einsum("ij,ij->i", civ, S) + ints.e_nuc
+        out["dav_opts"] = np.array([dav["krymin"], dav["krymax"], dav["nroots"],
+                                    dav["refdim"]])
+        out["energies"] = e
+        out["civec"] = civ
+        del H
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(name, ref.ndets, out.get("energies"))
+
+
+if __name__ == "__main__":
+    for n in (sys.argv[1:] or CASES):
+        make(n)
