@@ -171,6 +171,14 @@ jci_status jci_sigma_device(jci_space *s, int nvec, const void *v,
 jci_status jci_sigma_tuning(const jci_space *s, int precision, int *threads,
                             int *rows, float *ms);
 
+/* Fix the sigma plan instead of autotuning (for tests and measurements):
+ * mode 0 stages `rows` alpha-excitation rows per pass in one kernel, mode 1
+ * runs the alpha singles as a dense product in a second kernel; threads =
+ * 128/256/512/1024 per CTA of the row kernel.  Only for one-group (FCI/CAS)
+ * spaces after jci_set_integrals.  No reference counterpart. */
+jci_status jci_sigma_set_plan(jci_space *s, int precision, int mode,
+                              int threads, int rows);
+
 typedef struct {
         int maxiter;      /* &dalginfo defaults: 20 */
         int krymin;       /* 3 */

@@ -107,6 +107,7 @@ def lib():
                                    ctypes.POINTER(DavidsonStats)]
         L.jci_sigma_tuning.argtypes = [vp, ip, ctypes.POINTER(ip), ctypes.POINTER(ip),
                                        ctypes.POINTER(ctypes.c_float)]
+        L.jci_sigma_set_plan.argtypes = [vp, ip, ip, ip, ip]
         L.jci_read_namelists.argtypes = [ctypes.c_char_p, vp, vp, vp]
         L.jci_read_moints.argtypes = [ctypes.c_char_p, vp, ctypes.c_longlong, vp,
                                       ctypes.c_longlong, ctypes.POINTER(ip),
@@ -228,6 +229,11 @@ class Space:
         _check(lib().jci_sigma_tuning(self.h, precision, ctypes.byref(a), ctypes.byref(b),
                                       ctypes.byref(c)), "sigma_tuning")
         return a.value, b.value, c.value
+
+    def set_sigma_plan(self, precision, mode, threads, rows=1):
+        """Fix the FCI sigma plan (mode 0 staged rows, 1 dense product)."""
+        _check(lib().jci_sigma_set_plan(self.h, precision, mode, threads, rows),
+               "sigma_set_plan")
 
     def davidson(self, maxiter=500, krymin=4, krymax=12, nroots=1, prediagr=1,
                  refdim=8, restol=1e-8, precision=FP64, switch_tol=1e-4,

@@ -92,33 +92,37 @@ jci_status jci_sigma(jci_space *s, int nvec, const double *v, double *sig, int p
     if (!s->have_ints) return JCI_ERR_STATE;
     long long n = s->ndets;
     size_t w = precision == JCI_FP32 ? sizeof(float) : sizeof(double);
-    void *dv = nullptr, *ds = nullptr;
-    if (cudaMalloc(&dv, (size_t)nvec * n * w) != cudaSuccess) return JCI_ERR_NOMEM;
-    if (cudaMalloc(&ds, (size_t)nvec * n * w) != cudaSuccess) {
-        cudaFree(dv);
-        return JCI_ERR_NOMEM;
+    size_t bytes = (size_t)nvec * n * w;
+    DeviceState *d = s->dev;
+    cudaStream_t st = d->stream;
+    // staging buffers stay with the handle (grown on demand)
+    if (d->io_bytes < bytes) {
+        cudaFree(d->io_v);
+        cudaFree(d->io_s);
+        d->io_v = d->io_s = nullptr;
+        d->io_bytes = 0;
+        if (cudaMalloc(&d->io_v, bytes) != cudaSuccess) return JCI_ERR_NOMEM;
+        if (cudaMalloc(&d->io_s, bytes) != cudaSuccess) return JCI_ERR_NOMEM;
+        d->io_bytes = bytes;
     }
     jci_status r = JCI_OK;
     std::vector<float> tmp;
     if (precision == JCI_FP32) {
         tmp.resize((size_t)nvec * n);
         for (size_t i = 0; i < tmp.size(); i++) tmp[i] = (float)v[i];
-        if (cudaMemcpy(dv, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice)) r = JCI_ERR_CUDA;
-    } else if (cudaMemcpy(dv, v, (size_t)nvec * n * 8, cudaMemcpyHostToDevice)) {
+        if (cudaMemcpyAsync(d->io_v, tmp.data(), bytes, cudaMemcpyHostToDevice, st))
+            r = JCI_ERR_CUDA;
+    } else if (cudaMemcpyAsync(d->io_v, v, bytes, cudaMemcpyHostToDevice, st)) {
         r = JCI_ERR_CUDA;
     }
-    if (!r) r = device_sigma(s, nvec, dv, ds, n, precision, nullptr);
-    if (!r && cudaDeviceSynchronize() != cudaSuccess) r = JCI_ERR_CUDA;
+    if (!r) r = device_sigma(s, nvec, d->io_v, d->io_s, n, precision, nullptr);
     if (!r) {
-        if (precision == JCI_FP32) {
-            if (cudaMemcpy(tmp.data(), ds, tmp.size() * 4, cudaMemcpyDeviceToHost)) r = JCI_ERR_CUDA;
-            for (size_t i = 0; i < tmp.size() && !r; i++) sig[i] = tmp[i];
-        } else if (cudaMemcpy(sig, ds, (size_t)nvec * n * 8, cudaMemcpyDeviceToHost)) {
-            r = JCI_ERR_CUDA;
-        }
+        void *dst = precision == JCI_FP32 ? (void *)tmp.data() : (void *)sig;
+        if (cudaMemcpyAsync(dst, d->io_s, bytes, cudaMemcpyDeviceToHost, st)) r = JCI_ERR_CUDA;
     }
-    cudaFree(dv);
-    cudaFree(ds);
+    if (!r && cudaStreamSynchronize(st) != cudaSuccess) r = JCI_ERR_CUDA;
+    if (!r && precision == JCI_FP32)
+        for (size_t i = 0; i < tmp.size(); i++) sig[i] = tmp[i];
     return r;
 }
 
@@ -127,6 +131,13 @@ jci_status jci_sigma_tuning(const jci_space *s, int precision, int *threads, int
     if (!s || !threads || !rows || !ms) return JCI_ERR_ARG;
     fci_tuning(s, precision, threads, rows, ms);
     return JCI_OK;
+}
+
+jci_status jci_sigma_set_plan(jci_space *s, int precision, int mode, int threads, int rows) {
+    if (!s || (precision != JCI_FP64 && precision != JCI_FP32) || (mode != 0 && mode != 1))
+        return JCI_ERR_ARG;
+    if (!s->have_ints) return JCI_ERR_STATE;
+    return fci_force_plan(s, precision, mode, threads, rows);
 }
 
 void jci_davidson_defaults(jci_davidson_opts *o) {

@@ -166,7 +166,7 @@ void device_free(jci_space *s) {
         for (void *q : p) cudaFree(q);
     }
     void *p[] = {d->pairidx, d->pqoff, d->pqg, d->m1, d->m2, d->m1f, d->m2f, d->hd,
-                 d->hdf};
+                 d->hdf, d->io_v, d->io_s};
     for (void *q : p) cudaFree(q);
     fci_free(d);
     davidson_free(d);

@@ -58,6 +58,8 @@ struct DeviceState {
     float *hdf = nullptr;
     bool single_group = false;
     int *pqg = nullptr;            // npq x 2 group pair of each block
+    void *io_v = nullptr, *io_s = nullptr;  // host-API staging buffers
+    size_t io_bytes = 0;
     struct FciTables *fci = nullptr;   // single-group fast path (jci_fci.cu)
     struct DavidsonBuffers *dav = nullptr;  // jci_davidson.cu
 };

@@ -45,7 +45,10 @@ struct FciTables {
     FciSpin<float> f[2];
     size_t smem_max = 0;
     int tuned_nt[2] = {0, 0}, tuned_R[2] = {0, 0};  // per precision (autotuned)
+    int tuned_mode[2] = {0, 0};
     float tuned_ms[2] = {0.f, 0.f};
+    int mix_grid[2] = {0, 0};      // resident CTAs of k_sigma_mixed
+    void *tbuf[2] = {nullptr, nullptr};  // per-CTA product panels
 };
 
 bool fci_supported(const jci_space *s) {
@@ -61,6 +64,7 @@ void fci_free(DeviceState *d) {
         cudaFree(f->dblJ[s]);
         cudaFree(f->d[s].a1T); cudaFree(f->d[s].joccT); cudaFree(f->d[s].dblH);
         cudaFree(f->f[s].a1T); cudaFree(f->f[s].joccT); cudaFree(f->f[s].dblH);
+        cudaFree(f->tbuf[s]);
     }
     delete f;
     d->fci = nullptr;
@@ -102,6 +106,7 @@ __global__ void k_fci_tables(int nstr, int nelec, int ns, int nd, int npair,
 template <typename T>
 struct FciArgs {
     int na, nb, sa, sb, da, db, npair, R;
+    int do_as;                    // 0: alpha singles are left to k_sigma_mixed
     const uint32_t *fsA, *fsB;    // [single][string] target | sign << 31
     const uint16_t *fpA, *fpB;    // [single][string] pair index
     const T *a1A, *a1B;           // [single][string]
@@ -157,7 +162,7 @@ __global__ void __launch_bounds__(ITEMS <= 2 ? 1024 : 512)
     }
 
     // alpha singles (with alpha x beta doubles), R staged rows at a time
-    for (int e0 = 0; e0 < a.sa; e0 += a.R) {
+    for (int e0 = 0; a.do_as && e0 < a.sa; e0 += a.R) {
         const int nr = min(a.R, a.sa - e0);
         __syncthreads();
         if (tid < nr) {
@@ -223,6 +228,120 @@ __global__ void __launch_bounds__(ITEMS <= 2 ? 1024 : 512)
         int Ib = tid + it * nt;
         if (Ib < nb) dst[Ib] = acc[it];
     }
+}
+
+// ---- alpha singles and alpha x beta doubles as a dense product ------------
+//
+// For one alpha string Ia with alpha singles j -> (Ja_j, phase s_j, pair p_j):
+//   T[p][Jb] = sum_j A[p][j] c(Ja_j, Jb),   A[p][j] = s_j (p_j | p)
+//   T[U][Jb] = sum_j s_j a1(Ia, j) c(Ja_j, Jb)            (row U = npair)
+// then, for every beta string Ib,
+//   sigma(Ia, Ib) += T[U][Ib] + sum_{m in Ib} T[(mm)][Ib]
+//                  + sum_{beta singles Ib -> Jb, pair q, phase t} t T[q][Jb].
+// The first two terms are the alpha single elements (hmatels_1x with the
+// beta string's Coulomb sum sum_{m in Ib} (mm|p_j)); the last is
+// hmatels_2xab summed over both strings' singles.  The product runs on the
+// FP32/FP64 CUDA-core pipes with a 16x16 thread grid, each thread holding a
+// TM x 4 register tile; T goes to a per-CTA scratch panel in global memory
+// (L2-resident for the mid sizes) and is gathered back in a fixed order, so
+// results stay bitwise reproducible.
+
+constexpr int kMixThreads = 256;
+constexpr int kMixCols = 64;  // 16 threads x 4 columns per chunk
+
+template <typename T>
+struct MixArgs {
+    int na, nb, nbp, sa, sb, npair, mrows;
+    const uint32_t *fsA, *fsB;
+    const uint16_t *fpA, *fpB;
+    const T *a1A;
+    const T *m2;
+    const uint64_t *occB;
+};
+
+template <typename T, int TM>
+__global__ void __launch_bounds__(kMixThreads)
+    k_sigma_mixed(MixArgs<T> a, const T *__restrict__ V, T *__restrict__ S, T *__restrict__ Tbuf) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int MP = 16 * TM;
+    const int K = a.sa;
+    T *As = reinterpret_cast<T *>(smem_raw);          // [K][MP]
+    T *Bs = As + (size_t)K * MP;                      // [K][64]
+    int *jl = reinterpret_cast<int *>(Bs + (size_t)K * kMixCols);  // [K]
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    T *Tb = Tbuf + (size_t)blockIdx.x * a.mrows * a.nbp;
+    for (int Ia = blockIdx.x; Ia < a.na; Ia += gridDim.x) {
+        __syncthreads();
+        for (int idx = tid; idx < K * MP; idx += kMixThreads) {
+            int j = idx / MP, m = idx - j * MP;
+            long long o = (long long)j * a.na + Ia;
+            uint32_t e = a.fsA[o];
+            T v = T(0);
+            if (m < a.npair) v = a.m2[eri_index(a.fpA[o], m)];
+            else if (m == a.npair) v = a.a1A[o];
+            As[idx] = flip(v, e >> 31);
+            if (m == 0) jl[j] = (int)(e & 0x3fffffffu);
+        }
+        __syncthreads();
+        for (int c0 = 0; c0 < a.nbp; c0 += kMixCols) {
+            for (int idx = tid; idx < K * kMixCols; idx += kMixThreads) {
+                int j = idx >> 6, c = idx & 63, col = c0 + c;
+                Bs[idx] = col < a.nb ? V[(long long)jl[j] * a.nb + col] : T(0);
+            }
+            __syncthreads();
+            T acc[TM][4];
+#pragma unroll
+            for (int i = 0; i < TM; i++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) acc[i][q] = T(0);
+#pragma unroll 4
+            for (int k = 0; k < K; k++) {
+                const T *br = Bs + k * kMixCols + tx * 4;
+                T b0 = br[0], b1 = br[1], b2 = br[2], b3 = br[3];
+                const T *ar = As + k * MP + ty * TM;
+#pragma unroll
+                for (int i = 0; i < TM; i++) {
+                    T av = ar[i];
+                    acc[i][0] = fma(av, b0, acc[i][0]);
+                    acc[i][1] = fma(av, b1, acc[i][1]);
+                    acc[i][2] = fma(av, b2, acc[i][2]);
+                    acc[i][3] = fma(av, b3, acc[i][3]);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < TM; i++) {
+                int m = ty * TM + i;
+                if (m < a.mrows) {
+                    T *dst = Tb + (size_t)m * a.nbp + c0 + tx * 4;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) dst[q] = acc[i][q];
+                }
+            }
+            __syncthreads();
+        }
+        // gather: every column of the row owned by one thread, fixed order
+        const T *TU = Tb + (size_t)a.npair * a.nbp;
+        T *srow = S + (long long)Ia * a.nb;
+        for (int Ib = tid; Ib < a.nb; Ib += kMixThreads) {
+            T x = TU[Ib];
+            uint64_t oc = a.occB[Ib];
+            while (oc) {
+                int m = __ffsll((long long)oc);  // 1-based orbital
+                oc &= oc - 1;
+                x += Tb[(size_t)(m * (m + 1) / 2 - 1) * a.nbp + Ib];
+            }
+            for (int f = 0; f < a.sb; f++) {
+                long long o = (long long)f * a.nb + Ib;
+                uint32_t e = a.fsB[o];
+                x += flip(Tb[(size_t)a.fpB[o] * a.nbp + (e & 0x3fffffffu)], e >> 31);
+            }
+            srow[Ib] += x;
+        }
+    }
+}
+
+static size_t mix_smem(int K, int TM, size_t w) {
+    return (size_t)K * 16 * TM * w + (size_t)K * kMixCols * w + (size_t)K * 4 + 16;
 }
 
 static size_t fci_smem(int nb, int npair, int R, size_t w) {
@@ -303,8 +422,80 @@ static jci_status launch_one(const FciArgs<T> &a, int nt, size_t smem, int na, c
     return JCI_OK;
 }
 
-// Pick (threads per CTA, staged rows per pass) for this space by timing the
-// admissible candidates on scratch vectors; cached per precision.
+template <typename T>
+using MixKernel = void (*)(MixArgs<T>, const T *, T *, T *);
+
+template <typename T>
+static MixKernel<T> mixed_kernel(int TM) {
+    switch (TM) {
+        case 1: return k_sigma_mixed<T, 1>;
+        case 2: return k_sigma_mixed<T, 2>;
+        case 3: return k_sigma_mixed<T, 3>;
+        case 4: return k_sigma_mixed<T, 4>;
+        case 5: return k_sigma_mixed<T, 5>;
+        case 6: return k_sigma_mixed<T, 6>;
+        case 7: return k_sigma_mixed<T, 7>;
+        case 8: return k_sigma_mixed<T, 8>;
+        case 9: return k_sigma_mixed<T, 9>;
+        default: return nullptr;
+    }
+}
+
+static bool mixed_possible(const FciTables *f, size_t w) {
+    int mrows = f->npair + 1, TM = (mrows + 15) / 16;
+    return TM <= 9 && f->sa >= 1 && mix_smem(f->sa, TM, w) <= f->smem_max;
+}
+
+// Second kernel of the dense-product path; the per-CTA scratch panels are
+// allocated on first use (grid = resident CTAs on the whole device).
+template <typename T>
+static jci_status launch_mixed(jci_space *s, const FciArgs<T> &fa, const T *v, T *o,
+                               cudaStream_t st) {
+    DeviceState *d = s->dev;
+    FciTables *f = d->fci;
+    const int prec = sizeof(T) == 8 ? 0 : 1;
+    MixArgs<T> m;
+    m.na = fa.na; m.nb = fa.nb; m.nbp = (fa.nb + kMixCols - 1) / kMixCols * kMixCols;
+    m.sa = fa.sa; m.sb = fa.sb; m.npair = fa.npair; m.mrows = fa.npair + 1;
+    m.fsA = fa.fsA; m.fsB = fa.fsB; m.fpA = fa.fpA; m.fpB = fa.fpB;
+    m.a1A = fa.a1A; m.m2 = fa.m2; m.occB = d->t[1].occ;
+    int TM = (m.mrows + 15) / 16;
+    MixKernel<T> kern = mixed_kernel<T>(TM);
+    if (!kern) return JCI_ERR_SPACE;
+    size_t smem = mix_smem(m.sa, TM, sizeof(T));
+    if (!f->mix_grid[prec]) {
+        JCI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        int occ = 0, nsm = 0;
+        JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kMixThreads, smem));
+        JCI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d->device));
+        int grid = std::max(1, std::min(m.na, nsm * std::max(occ, 1)));
+        size_t bytes = (size_t)grid * m.mrows * m.nbp * sizeof(T);
+        JCI_CUDA(cudaMalloc(&f->tbuf[prec], bytes));
+        f->mix_grid[prec] = grid;
+    }
+    kern<<<f->mix_grid[prec], kMixThreads, smem, st>>>(m, v, o, (T *)f->tbuf[prec]);
+    return JCI_OK;
+}
+
+// One full sigma of one vector with the given plan.
+template <typename T>
+static jci_status run_plan(jci_space *s, FciArgs<T> a, int mode, int nt, int R, const T *v, T *o,
+                           cudaStream_t st) {
+    FciTables *f = s->dev->fci;
+    size_t w = sizeof(T);
+    a.do_as = mode == 0;
+    a.R = mode == 0 ? R : 0;
+    jci_status r = launch_one<T>(a, nt, fci_smem(f->nb, f->npair, a.R, w), f->na, v, o, st);
+    if (r) return r;
+    if (mode == 1) return launch_mixed<T>(s, a, v, o, st);
+    return JCI_OK;
+}
+
+// Pick the plan for this space by timing the admissible candidates on
+// scratch vectors: mode 0 stages R alpha rows per pass in one kernel, mode 1
+// runs the alpha singles as the dense product above; nt = threads per CTA
+// of the row kernel.  Cached per precision.
 template <typename T>
 static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     DeviceState *d = s->dev;
@@ -317,34 +508,37 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     JCI_CUDA(cudaMalloc(&o, n * w));
     JCI_CUDA(cudaMemsetAsync(v, 0, n * w, st));
     float best = 1e30f;
-    int bnt = 0, bR = 0;
+    int bnt = 0, bR = 0, bmode = 0;
     const int nts[] = {128, 256, 512, 1024};
     const int Rs[] = {1, 2, 4, 8, 16};
     cudaEvent_t e0, e1;
     JCI_CUDA(cudaEventCreate(&e0));
     JCI_CUDA(cudaEventCreate(&e1));
-    for (int nt : nts) {
-        int items = (f->nb + nt - 1) / nt;
-        if (items > 32 || (nt == 1024 && items > 2)) continue;
-        if (nt > 32 * ((f->nb + 31) / 32) && nt > 128) continue;  // idle threads
-        for (int R : Rs) {
-            if (R > f->sa && R > 1) continue;
-            size_t smem = fci_smem(f->nb, f->npair, R, w);
-            if (smem > f->smem_max) continue;
-            a.R = R;
-            jci_status r = launch_one<T>(a, nt, smem, f->na, v, o, st);
-            if (r) return r;
-            JCI_CUDA(cudaEventRecord(e0, st));
-            for (int k = 0; k < 2; k++)
-                if ((r = launch_one<T>(a, nt, smem, f->na, v, o, st))) return r;
-            JCI_CUDA(cudaEventRecord(e1, st));
-            JCI_CUDA(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            JCI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best) {
-                best = ms;
-                bnt = nt;
-                bR = R;
+    for (int mode = 0; mode < 2; mode++) {
+        if (mode == 1 && !mixed_possible(f, w)) continue;
+        for (int nt : nts) {
+            int items = (f->nb + nt - 1) / nt;
+            if (items > 32 || (nt == 1024 && items > 2)) continue;
+            if (nt > 32 * ((f->nb + 31) / 32) && nt > 128) continue;  // idle threads
+            for (int R : Rs) {
+                if (mode == 1 && R != 1) continue;
+                if (mode == 0 && R > f->sa && R > 1) continue;
+                if (fci_smem(f->nb, f->npair, mode == 0 ? R : 0, w) > f->smem_max) continue;
+                jci_status r = run_plan<T>(s, a, mode, nt, R, v, o, st);
+                if (r) return r;
+                JCI_CUDA(cudaEventRecord(e0, st));
+                for (int k = 0; k < 2; k++)
+                    if ((r = run_plan<T>(s, a, mode, nt, R, v, o, st))) return r;
+                JCI_CUDA(cudaEventRecord(e1, st));
+                JCI_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                JCI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best) {
+                    best = ms;
+                    bnt = nt;
+                    bR = R;
+                    bmode = mode;
+                }
             }
         }
     }
@@ -355,6 +549,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     if (!bnt) return JCI_ERR_SPACE;
     f->tuned_nt[prec] = bnt;
     f->tuned_R[prec] = bR;
+    f->tuned_mode[prec] = bmode;
     f->tuned_ms[prec] = best / 2;
     return JCI_OK;
 }
@@ -363,7 +558,8 @@ void fci_tuning(const jci_space *s, int precision, int *nt, int *R, float *ms) {
     const FciTables *f = s->dev ? s->dev->fci : nullptr;
     int p = precision == JCI_FP32 ? 1 : 0;
     *nt = f ? f->tuned_nt[p] : 0;
-    *R = f ? f->tuned_R[p] : 0;
+    // rows staged per pass; 0 when the alpha singles run as the dense product
+    *R = f ? (f->tuned_mode[p] == 1 ? 0 : f->tuned_R[p]) : 0;
     *ms = f ? f->tuned_ms[p] : 0.f;
 }
 
@@ -376,6 +572,8 @@ static jci_status launch_fci(jci_space *s, int nvec, const T *V, T *S, long long
     FciArgs<T> a;
     a.na = f->na; a.nb = f->nb; a.sa = f->sa; a.sb = f->sb; a.da = f->da; a.db = f->db;
     a.npair = f->npair;
+    a.R = 1;
+    a.do_as = 1;
     a.fsA = d->t[0].fsing; a.fsB = d->t[1].fsing;
     a.fpA = d->t[0].fspair; a.fpB = d->t[1].fspair;
     a.dJA = f->dblJ[0]; a.dJB = f->dblJ[1];
@@ -390,16 +588,13 @@ static jci_status launch_fci(jci_space *s, int nvec, const T *V, T *S, long long
         a.dHA = (const T *)f->f[0].dblH; a.dHB = (const T *)f->f[1].dblH;
         a.hd = (const T *)d->hdf; a.m2 = (const T *)d->m2f;
     }
-    size_t w = sizeof(T);
-    int &nt = f->tuned_nt[prec], &R = f->tuned_R[prec];
-    if (nt == 0) {
+    if (f->tuned_nt[prec] == 0) {
         jci_status r = autotune<T>(s, a, st);
         if (r) return r;
     }
-    a.R = R;
     for (int c = 0; c < nvec; c++) {
-        jci_status r = launch_one<T>(a, nt, fci_smem(f->nb, f->npair, R, w), f->na,
-                                     V + c * ld, S + c * ld, st);
+        jci_status r = run_plan<T>(s, a, f->tuned_mode[prec], f->tuned_nt[prec],
+                                   f->tuned_R[prec], V + c * ld, S + c * ld, st);
         if (r) return r;
     }
     JCI_CUDA(cudaGetLastError());
@@ -413,4 +608,23 @@ jci_status fci_sigma(jci_space *s, int nvec, const void *v, void *sig, long long
     return launch_fci<double>(s, nvec, (const double *)v, (double *)sig, ld, st);
 }
 
+// Force a plan (mode 0: staged rows R, mode 1: dense product) for tests and
+// measurements; nt = threads per CTA of the row kernel.
+jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R) {
+    FciTables *f = s->dev ? s->dev->fci : nullptr;
+    if (!f) return JCI_ERR_STATE;
+    int p = precision == JCI_FP32 ? 1 : 0;
+    size_t w = p ? sizeof(float) : sizeof(double);
+    if (mode == 1 && !mixed_possible(f, w)) return JCI_ERR_ARG;
+    int items = (f->nb + nt - 1) / nt;
+    if ((nt != 128 && nt != 256 && nt != 512 && nt != 1024) || items > 32 ||
+        (nt == 1024 && items > 2))
+        return JCI_ERR_ARG;
+    if (mode == 0 && (R < 1 || fci_smem(f->nb, f->npair, R, w) > f->smem_max)) return JCI_ERR_ARG;
+    f->tuned_mode[p] = mode;
+    f->tuned_nt[p] = nt;
+    f->tuned_R[p] = mode == 0 ? R : 1;
+    f->tuned_ms[p] = 0.f;
+    return JCI_OK;
+}
 }  // namespace jci

@@ -14,6 +14,7 @@ jci_status fci_sigma(jci_space *s, int nvec, const void *v, void *sig, long long
                      int precision, cudaStream_t st);
 void fci_free(DeviceState *d);
 void fci_tuning(const jci_space *s, int precision, int *nt, int *R, float *ms);
+jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R);
 
 // Generic path (any truncated space), jci_device.cu.
 jci_status device_sigma_generic(jci_space *s, int nvec, const void *vin, void *sout,

@@ -172,3 +172,27 @@ def test_pdavidson_drop_in(name, tmp_path, monkeypatch):
     civ = jb.read_vectors("civec", nroots, ndets)
     ov = np.abs(np.einsum("ij,ij->i", civ, g["civec"]))
     assert (ov > 1 - 1e-9).all()
+
+
+def test_jci_program_end_to_end(tmp_path):
+    """The jci driver reads jayci.in + a SIFS moints file like pjayci and
+    writes civec (execute_pjayci.c flow on one GPU)."""
+    import subprocess
+    g = load("cas6_6")
+    kmin, kmax, nroots, refdim = (int(x) for x in g["dav_opts"])
+    (tmp_path / "jayci.in").write_text(
+        f" &general\n electrons=6, orbitals=6, nfrozen=0, ndocc=0, nactive=6, xlevel=0\n /\n"
+        f" &dalginfo\n maxiter=500, krymin={kmin}, krymax={kmax}, nroots={nroots},\n"
+        f" prediagr=1, restol=1.0d-9, refdim={refdim}\n /\n &gpuinfo exactrestol=1 /\n")
+    jb.write_moints(tmp_path / "moints", 6, g["m1"], g["m2"], float(g["e_nuc"]), 0.0)
+    exe = os.path.join(os.path.dirname(jb.LIBPATH), "jci")
+    if not os.path.exists(exe):
+        from jayci_b200 import build
+        build.build()
+    r = subprocess.run([exe], cwd=tmp_path, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    e = [float(l.split()[-1]) for l in r.stdout.splitlines() if "Root #" in l]
+    np.testing.assert_allclose(e, g["energies"], atol=1e-10)
+    civ = jb.read_vectors(str(tmp_path / "civec"), nroots, 400)
+    ov = np.abs(np.einsum("ij,ij->i", civ, g["civec"]))
+    assert (ov > 1 - 1e-9).all()
