@@ -164,6 +164,27 @@ jci_status jci_sigma_device(jci_space *s, int nvec, const void *v,
                             void *sigma, long long ld, int precision,
                             void *stream);
 
+/* sigma = H v for ONE device vector (ld = ndets) that allocates no device
+ * memory, for callers that cannot call cudaMalloc while they run sigma
+ * (a driver capturing its iteration into a CUDA graph, a process under a
+ * fixed device-memory budget, an application whose allocator forbids
+ * cudaMalloc / cudaFree after start-up).  The alpha-singles product kernel
+ * keeps its per-CTA panels in a fixed device array of 64 MiB that lives in
+ * the library (every GPU that loads libjci holds it until exit) instead of
+ * a buffer allocated on first use; jci_set_integrals must have been called
+ * before (it builds the tables this call reads).  One-group (FCI / CAS)
+ * spaces only; returns JCI_ERR_SPACE when one alpha row's panel,
+ * (n(n+1)/2 + 1) x Nbeta rounded up to 64 elements, exceeds 64 MiB.  The
+ * first call on a device looks up the array's device address (once per
+ * device, with that device current); make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * streams, other host threads, other handles on the same device) race and
+ * must be serialised by the caller.  Nothing in the array needs clearing: a
+ * call writes every panel element before reading it.  No counterpart in the
+ * reference (which has no device code). */
+jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sigma,
+                                    int precision, void *stream);
+
 /* Launch shape the sigma autotuner picked for this space (threads per CTA
  * and alpha rows staged per pass; both 0 before the first sigma call or on
  * the multi-group path) and its timed cost in ms per vector.  No reference

@@ -133,6 +133,15 @@ jci_status jci_sigma_tuning(const jci_space *s, int precision, int *threads, int
     return JCI_OK;
 }
 
+jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sig, int precision,
+                                    void *stream) {
+    if (!s || !v || !sig) return JCI_ERR_ARG;
+    if (precision != JCI_FP64 && precision != JCI_FP32) return JCI_ERR_ARG;
+    if (!s->have_ints || !s->dev) return JCI_ERR_STATE;
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->dev->stream;
+    return fci_sigma_noalloc(s, v, sig, precision, st);
+}
+
 jci_status jci_sigma_set_plan(jci_space *s, int precision, int mode, int threads, int rows) {
     if (!s || (precision != JCI_FP64 && precision != JCI_FP32) || (mode != 0 && mode != 1))
         return JCI_ERR_ARG;

@@ -25,6 +25,7 @@
 // result is bitwise reproducible run to run.
 #include <algorithm>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "jci_kernels.cuh"
@@ -627,4 +628,102 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R) 
     f->tuned_ms[p] = 0.f;
     return JCI_OK;
 }
+
+// ---- allocation-free sigma ----------------------------------------------
+//
+// For callers that cannot allocate device memory while they run sigma: a
+// driver that captures its whole iteration into a CUDA graph, a host that
+// runs under a fixed device-memory budget, or an embedding application
+// whose allocator forbids cudaMalloc / cudaFree after start-up.  The
+// dense-product kernel's per-CTA panels come from this fixed, statically
+// sized device array instead of a buffer allocated on first use; the
+// tables built by jci_set_integrals are reused as they are.
+
+constexpr size_t kNoAllocScratchBytes = 64ull << 20;  // 64 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+static void *g_noalloc_ptr[kMaxDevices];
+static std::once_flag g_noalloc_once[kMaxDevices];
+static cudaError_t g_noalloc_err[kMaxDevices];
+
+// Device address of g_noalloc_scratch on the current device.  The host-side
+// name is only a stand-in for the symbol, so the address is looked up once
+// per device (with that device current) and cached.
+static jci_status noalloc_scratch(int dev, void **out) {
+    if (dev < 0 || dev >= kMaxDevices) return JCI_ERR_ARG;
+    std::call_once(g_noalloc_once[dev], [dev]() {
+        g_noalloc_err[dev] = cudaGetSymbolAddress(&g_noalloc_ptr[dev], g_noalloc_scratch);
+    });
+    if (g_noalloc_err[dev] != cudaSuccess)
+        return cuda_fail(g_noalloc_err[dev], "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__,
+                         __LINE__);
+    *out = g_noalloc_ptr[dev];
+    return JCI_OK;
+}
+
+template <typename T>
+static jci_status sigma_noalloc(jci_space *s, const T *v, T *o, cudaStream_t st) {
+    DeviceState *d = s->dev;
+    FciTables *f = d->fci;
+    const int prec = sizeof(T) == 8 ? 0 : 1;
+    size_t w = sizeof(T);
+    if (!mixed_possible(f, w)) return JCI_ERR_SPACE;
+    FciArgs<T> a;
+    a.na = f->na; a.nb = f->nb; a.sa = f->sa; a.sb = f->sb; a.da = f->da; a.db = f->db;
+    a.npair = f->npair;
+    a.R = 0;
+    a.do_as = 0;
+    a.fsA = d->t[0].fsing; a.fsB = d->t[1].fsing;
+    a.fpA = d->t[0].fspair; a.fpB = d->t[1].fspair;
+    a.dJA = f->dblJ[0]; a.dJB = f->dblJ[1];
+    if (prec == 0) {
+        a.a1A = (const T *)f->d[0].a1T; a.a1B = (const T *)f->d[1].a1T;
+        a.jA = (const T *)f->d[0].joccT; a.jB = (const T *)f->d[1].joccT;
+        a.dHA = (const T *)f->d[0].dblH; a.dHB = (const T *)f->d[1].dblH;
+        a.hd = (const T *)d->hd; a.m2 = (const T *)d->m2;
+    } else {
+        a.a1A = (const T *)f->f[0].a1T; a.a1B = (const T *)f->f[1].a1T;
+        a.jA = (const T *)f->f[0].joccT; a.jB = (const T *)f->f[1].joccT;
+        a.dHA = (const T *)f->f[0].dblH; a.dHB = (const T *)f->f[1].dblH;
+        a.hd = (const T *)d->hdf; a.m2 = (const T *)d->m2f;
+    }
+    MixArgs<T> m;
+    m.na = a.na; m.nb = a.nb; m.nbp = (a.nb + kMixCols - 1) / kMixCols * kMixCols;
+    m.sa = a.sa; m.sb = a.sb; m.npair = a.npair; m.mrows = a.npair + 1;
+    m.fsA = a.fsA; m.fsB = a.fsB; m.fpA = a.fpA; m.fpB = a.fpB;
+    m.a1A = a.a1A; m.m2 = a.m2; m.occB = d->t[1].occ;
+    size_t panel = (size_t)m.mrows * m.nbp * w;
+    if (panel > kNoAllocScratchBytes) return JCI_ERR_SPACE;  // one row's panel must fit
+    int TM = (m.mrows + 15) / 16;
+    MixKernel<T> kern = mixed_kernel<T>(TM);
+    if (!kern) return JCI_ERR_SPACE;
+    void *scratch = nullptr;
+    jci_status r = noalloc_scratch(d->device, &scratch);
+    if (r) return r;
+    // row kernel: the tuned thread count if there is one, else a fixed shape
+    int nt = f->tuned_nt[prec] ? f->tuned_nt[prec] : (a.nb > 2048 ? 512 : 256);
+    if ((r = launch_one<T>(a, nt, fci_smem(a.nb, a.npair, 0, w), a.na, v, o, st))) return r;
+    size_t smem = mix_smem(m.sa, TM, w);
+    JCI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0, nsm = 0;
+    JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kMixThreads, smem));
+    JCI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d->device));
+    int grid = (int)std::min<size_t>(kNoAllocScratchBytes / panel,
+                                     (size_t)nsm * std::max(occ, 1));
+    grid = std::max(1, std::min(grid, m.na));
+    kern<<<grid, kMixThreads, smem, st>>>(m, v, o, (T *)scratch);
+    JCI_CUDA(cudaGetLastError());
+    return JCI_OK;
+}
+
+jci_status fci_sigma_noalloc(jci_space *s, const void *v, void *o, int precision,
+                             cudaStream_t st) {
+    if (!s->dev || !s->dev->fci || !s->dev->single_group) return JCI_ERR_SPACE;
+    if (precision == JCI_FP32) return sigma_noalloc<float>(s, (const float *)v, (float *)o, st);
+    return sigma_noalloc<double>(s, (const double *)v, (double *)o, st);
+}
+
+size_t fci_noalloc_scratch_bytes() { return kNoAllocScratchBytes; }
+
 }  // namespace jci

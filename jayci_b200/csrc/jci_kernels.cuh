@@ -15,6 +15,9 @@ jci_status fci_sigma(jci_space *s, int nvec, const void *v, void *sig, long long
 void fci_free(DeviceState *d);
 void fci_tuning(const jci_space *s, int precision, int *nt, int *R, float *ms);
 jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R);
+jci_status fci_sigma_noalloc(jci_space *s, const void *v, void *o, int precision,
+                             cudaStream_t st);
+size_t fci_noalloc_scratch_bytes();
 
 // Generic path (any truncated space), jci_device.cu.
 jci_status device_sigma_generic(jci_space *s, int nvec, const void *vin, void *sout,
