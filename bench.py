@@ -316,7 +316,7 @@ def run_gpu(a):
                    "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"reference sigma (compute_cblock_Hfastest), {nvec} vectors, "
                              f"{sample}, OMP_SCHEDULE=dynamic,64"}
-    nt, R, _ = sp.sigma_tuning(jb.FP64)
+    mode, nt, R, B, _ = sp.sigma_tuning(jb.FP64)
     out = {"metric": METRIC, "value": value, "unit": "Gdet/s", "n_gpus": world,
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": tot_ms / a.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -324,11 +324,15 @@ def run_gpu(a):
            "config": {"workload": a.workload, "ndets": N, "vectors_per_step": nvec,
                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                       "l2": "flushed (256 MiB write) before every step",
-                      "sigma_launch": {"threads": nt, "staged_rows": R}},
+                      "sigma_plan": {"mode": ["staged rows", "dense product, global panel",
+                                              "dense product, shared-memory panel"][mode],
+                                     "row_kernel_threads": nt,
+                                     ("staged_rows" if mode == 0 else "product_ctas_per_sm"): R,
+                                     "rows_per_cta": B}},
            "roofline": roof, "cpu_baseline": cpu,
            "e2e": {"value": e2e, "unit": "Gdet/s", "h2d_bytes_per_step": nvec * N * 8,
                    "d2h_bytes_per_step": nvec * N * 8},
-           "gpu_launches": a.steps * nvec,
+           "gpu_launches": a.steps * nvec * (2 if mode >= 1 else 1),
            "clocks": clk,
            "fp32_sigma_gdet_s": value32,
            "solves": solves}

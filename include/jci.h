@@ -185,20 +185,27 @@ jci_status jci_sigma_device(jci_space *s, int nvec, const void *v,
 jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sigma,
                                     int precision, void *stream);
 
-/* Launch shape the sigma autotuner picked for this space (threads per CTA
- * and alpha rows staged per pass; both 0 before the first sigma call or on
- * the multi-group path) and its timed cost in ms per vector.  No reference
- * counterpart (the reference has no device tuning). */
-jci_status jci_sigma_tuning(const jci_space *s, int precision, int *threads,
-                            int *rows, float *ms);
+/* Plan the sigma autotuner picked for this space: mode (0 staged rows,
+ * 1 dense product with a global scratch panel, 2 dense product consumed
+ * from shared memory), threads per CTA of the row kernel, `rows` (mode 0:
+ * alpha rows staged per pass; modes 1-2: product-kernel CTAs per SM, 0 = as
+ * many as fit), `batch` (modes 1-2: alpha strings per CTA of the row kernel),
+ * and its timed cost in ms per vector.  All 0 before the first sigma call
+ * and on the multi-group path.  No reference counterpart (the reference
+ * has no device tuning). */
+jci_status jci_sigma_tuning(const jci_space *s, int precision, int *mode,
+                            int *threads, int *rows, int *batch, float *ms);
 
 /* Fix the sigma plan instead of autotuning (for tests and measurements):
- * mode 0 stages `rows` alpha-excitation rows per pass in one kernel, mode 1
- * runs the alpha singles as a dense product in a second kernel; threads =
- * 128/256/512/1024 per CTA of the row kernel.  Only for one-group (FCI/CAS)
- * spaces after jci_set_integrals.  No reference counterpart. */
+ * mode 0 stages `rows` alpha-excitation rows per pass in one kernel; modes
+ * 1 and 2 run a row kernel with `batch` (1, 2, 4) alpha strings per CTA and
+ * then the alpha singles as a dense product with `rows` CTAs per SM (0 = as
+ * many as fit), through a global panel (1) or shared memory (2); threads =
+ * 128/256/512/1024 per CTA of the row kernel.  Only for
+ * one-group (FCI/CAS) spaces after jci_set_integrals.  No reference
+ * counterpart. */
 jci_status jci_sigma_set_plan(jci_space *s, int precision, int mode,
-                              int threads, int rows);
+                              int threads, int rows, int batch);
 
 typedef struct {
         int maxiter;      /* &dalginfo defaults: 20 */

@@ -106,8 +106,9 @@ def lib():
         L.jci_davidson.argtypes = [vp, ctypes.POINTER(DavidsonOpts), vp, vp,
                                    ctypes.POINTER(DavidsonStats)]
         L.jci_sigma_tuning.argtypes = [vp, ip, ctypes.POINTER(ip), ctypes.POINTER(ip),
+                                       ctypes.POINTER(ip), ctypes.POINTER(ip),
                                        ctypes.POINTER(ctypes.c_float)]
-        L.jci_sigma_set_plan.argtypes = [vp, ip, ip, ip, ip]
+        L.jci_sigma_set_plan.argtypes = [vp, ip, ip, ip, ip, ip]
         L.jci_read_namelists.argtypes = [ctypes.c_char_p, vp, vp, vp]
         L.jci_read_moints.argtypes = [ctypes.c_char_p, vp, ctypes.c_longlong, vp,
                                       ctypes.c_longlong, ctypes.POINTER(ip),
@@ -224,15 +225,19 @@ class Space:
                                       ctypes.c_void_p(stream or 0)), "sigma_device")
 
     def sigma_tuning(self, precision=FP64):
-        """(threads per CTA, staged rows, ms per vector) chosen by the autotuner."""
-        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
-        _check(lib().jci_sigma_tuning(self.h, precision, ctypes.byref(a), ctypes.byref(b),
-                                      ctypes.byref(c)), "sigma_tuning")
-        return a.value, b.value, c.value
+        """(mode, threads, rows, batch, ms per vector) chosen by the autotuner;
+        rows = staged alpha rows (mode 0) or product CTAs per SM (mode 1),
+        batch = alpha strings per CTA of the mode-1 row kernel."""
+        m, a, b, g, c = (ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int(),
+                         ctypes.c_float())
+        _check(lib().jci_sigma_tuning(self.h, precision, ctypes.byref(m), ctypes.byref(a),
+                                      ctypes.byref(b), ctypes.byref(g), ctypes.byref(c)),
+               "sigma_tuning")
+        return m.value, a.value, b.value, g.value, c.value
 
-    def set_sigma_plan(self, precision, mode, threads, rows=1):
+    def set_sigma_plan(self, precision, mode, threads, rows=1, batch=1):
         """Fix the FCI sigma plan (mode 0 staged rows, 1 dense product)."""
-        _check(lib().jci_sigma_set_plan(self.h, precision, mode, threads, rows),
+        _check(lib().jci_sigma_set_plan(self.h, precision, mode, threads, rows, batch),
                "sigma_set_plan")
 
     def davidson(self, maxiter=500, krymin=4, krymax=12, nroots=1, prediagr=1,

@@ -126,10 +126,10 @@ jci_status jci_sigma(jci_space *s, int nvec, const double *v, double *sig, int p
     return r;
 }
 
-jci_status jci_sigma_tuning(const jci_space *s, int precision, int *threads, int *rows,
-                            float *ms) {
-    if (!s || !threads || !rows || !ms) return JCI_ERR_ARG;
-    fci_tuning(s, precision, threads, rows, ms);
+jci_status jci_sigma_tuning(const jci_space *s, int precision, int *mode, int *threads,
+                            int *rows, int *batch, float *ms) {
+    if (!s || !mode || !threads || !rows || !batch || !ms) return JCI_ERR_ARG;
+    fci_tuning(s, precision, mode, threads, rows, batch, ms);
     return JCI_OK;
 }
 
@@ -142,11 +142,12 @@ jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sig, int 
     return fci_sigma_noalloc(s, v, sig, precision, st);
 }
 
-jci_status jci_sigma_set_plan(jci_space *s, int precision, int mode, int threads, int rows) {
-    if (!s || (precision != JCI_FP64 && precision != JCI_FP32) || (mode != 0 && mode != 1))
+jci_status jci_sigma_set_plan(jci_space *s, int precision, int mode, int threads, int rows,
+                              int batch) {
+    if (!s || (precision != JCI_FP64 && precision != JCI_FP32) || mode < 0 || mode > 2)
         return JCI_ERR_ARG;
     if (!s->have_ints) return JCI_ERR_STATE;
-    return fci_force_plan(s, precision, mode, threads, rows);
+    return fci_force_plan(s, precision, mode, threads, rows, batch);
 }
 
 void jci_davidson_defaults(jci_davidson_opts *o) {

@@ -25,6 +25,8 @@
 // result is bitwise reproducible run to run.
 #include <algorithm>
 #include <cstdio>
+#include <cuda_pipeline.h>
+
 #include <mutex>
 #include <vector>
 
@@ -46,10 +48,12 @@ struct FciTables {
     FciSpin<float> f[2];
     size_t smem_max = 0;
     int tuned_nt[2] = {0, 0}, tuned_R[2] = {0, 0};  // per precision (autotuned)
-    int tuned_mode[2] = {0, 0};
+    int tuned_mode[2] = {0, 0}, tuned_B[2] = {1, 1};
     float tuned_ms[2] = {0.f, 0.f};
     int mix_grid[2] = {0, 0};      // resident CTAs of k_sigma_mixed
+    int mix_occ[2] = {1, 1}, nsm = 0;
     void *tbuf[2] = {nullptr, nullptr};  // per-CTA product panels
+    uint32_t *sortB = nullptr;     // [Ib][f] beta singles sorted by target
 };
 
 bool fci_supported(const jci_space *s) {
@@ -67,6 +71,7 @@ void fci_free(DeviceState *d) {
         cudaFree(f->f[s].a1T); cudaFree(f->f[s].joccT); cudaFree(f->f[s].dblH);
         cudaFree(f->tbuf[s]);
     }
+    cudaFree(f->sortB);
     delete f;
     d->fci = nullptr;
 }
@@ -267,10 +272,24 @@ __global__ void __launch_bounds__(kMixThreads)
     constexpr int MP = 16 * TM;
     const int K = a.sa;
     T *As = reinterpret_cast<T *>(smem_raw);          // [K][MP]
-    T *Bs = As + (size_t)K * MP;                      // [K][64]
-    int *jl = reinterpret_cast<int *>(Bs + (size_t)K * kMixCols);  // [K]
+    T *Bs = As + (size_t)K * MP;                      // [2][K][64]
+    int *jl = reinterpret_cast<int *>(Bs + 2 * (size_t)K * kMixCols);  // [K]
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     T *Tb = Tbuf + (size_t)blockIdx.x * a.mrows * a.nbp;
+    const int nchunk = a.nbp / kMixCols;
+    // B chunks are double-buffered: chunk c+1 is copied (cp.async) while
+    // chunk c is multiplied
+    auto stage = [&](int c, T *buf) {
+        const int c0 = c * kMixCols;
+        for (int idx = tid; idx < K * kMixCols; idx += kMixThreads) {
+            int j = idx >> 6, col = c0 + (idx & 63);
+            if (col < a.nb)
+                __pipeline_memcpy_async(buf + idx, V + (long long)jl[j] * a.nb + col, sizeof(T));
+            else
+                buf[idx] = T(0);
+        }
+        __pipeline_commit();
+    };
     for (int Ia = blockIdx.x; Ia < a.na; Ia += gridDim.x) {
         __syncthreads();
         for (int idx = tid; idx < K * MP; idx += kMixThreads) {
@@ -284,10 +303,15 @@ __global__ void __launch_bounds__(kMixThreads)
             if (m == 0) jl[j] = (int)(e & 0x3fffffffu);
         }
         __syncthreads();
-        for (int c0 = 0; c0 < a.nbp; c0 += kMixCols) {
-            for (int idx = tid; idx < K * kMixCols; idx += kMixThreads) {
-                int j = idx >> 6, c = idx & 63, col = c0 + c;
-                Bs[idx] = col < a.nb ? V[(long long)jl[j] * a.nb + col] : T(0);
+        stage(0, Bs);
+        for (int ci = 0; ci < nchunk; ci++) {
+            const int c0 = ci * kMixCols;
+            T *Bc = Bs + (size_t)(ci & 1) * K * kMixCols;
+            if (ci + 1 < nchunk) {
+                stage(ci + 1, Bs + (size_t)((ci + 1) & 1) * K * kMixCols);
+                __pipeline_wait_prior(1);
+            } else {
+                __pipeline_wait_prior(0);
             }
             __syncthreads();
             T acc[TM][4];
@@ -297,8 +321,10 @@ __global__ void __launch_bounds__(kMixThreads)
                 for (int q = 0; q < 4; q++) acc[i][q] = T(0);
 #pragma unroll 4
             for (int k = 0; k < K; k++) {
-                const T *br = Bs + k * kMixCols + tx * 4;
-                T b0 = br[0], b1 = br[1], b2 = br[2], b3 = br[3];
+                // thread tx owns columns tx, tx+16, tx+32, tx+48: a warp
+                // reads 16 consecutive words per load (no bank conflicts)
+                const T *br = Bc + k * kMixCols + tx;
+                T b0 = br[0], b1 = br[16], b2 = br[32], b3 = br[48];
                 const T *ar = As + k * MP + ty * TM;
 #pragma unroll
                 for (int i = 0; i < TM; i++) {
@@ -313,9 +339,9 @@ __global__ void __launch_bounds__(kMixThreads)
             for (int i = 0; i < TM; i++) {
                 int m = ty * TM + i;
                 if (m < a.mrows) {
-                    T *dst = Tb + (size_t)m * a.nbp + c0 + tx * 4;
+                    T *dst = Tb + (size_t)m * a.nbp + c0 + tx;
 #pragma unroll
-                    for (int q = 0; q < 4; q++) dst[q] = acc[i][q];
+                    for (int q = 0; q < 4; q++) dst[16 * q] = acc[i][q];
                 }
             }
             __syncthreads();
@@ -341,8 +367,233 @@ __global__ void __launch_bounds__(kMixThreads)
     }
 }
 
+// ---- dense product without a global panel ---------------------------------
+//
+// Same product as k_sigma_mixed, but each 64-column chunk of T is kept in
+// shared memory and consumed at once: every beta string Ib walks its singles
+// sorted by target (sortB, J | pair << 16 | sign << 31) and adds the entries
+// whose target falls in the current chunk; the one-body and Coulomb rows are
+// added when the chunk holds Ib itself.  Per-string accumulators and walk
+// positions live in shared memory, one owner thread per string, so the sums
+// are taken in a fixed order (bitwise reproducible) and T never leaves the SM.
+
+template <typename T>
+struct Mix2Args {
+    int na, nb, nbp, sa, sb, npair, mrows;
+    const uint32_t *fsA;
+    const uint16_t *fpA;
+    const uint32_t *sortB;   // [Ib][f] sorted by target
+    const T *a1A;
+    const T *m2;
+    const uint64_t *occB;
+};
+
+template <typename T, int TM>
+__global__ void __launch_bounds__(kMixThreads)
+    k_sigma_mixed2(Mix2Args<T> a, const T *__restrict__ V, T *__restrict__ S) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int MP = 16 * TM;
+    const int K = a.sa, nb = a.nb;
+    T *As = reinterpret_cast<T *>(smem_raw);          // [K][MP]
+    T *Bs = As + (size_t)K * MP;                      // [2][K][64]
+    T *Ts = Bs + 2 * (size_t)K * kMixCols;            // [mrows][64]
+    T *accs = Ts + (size_t)a.mrows * kMixCols;        // [nb]
+    int *jl = reinterpret_cast<int *>(accs + nb);     // [K]
+    unsigned char *pos = reinterpret_cast<unsigned char *>(jl + K);  // [nb]
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int nchunk = a.nbp / kMixCols;
+    auto stage = [&](int c, T *buf) {
+        const int c0 = c * kMixCols;
+        for (int idx = tid; idx < K * kMixCols; idx += kMixThreads) {
+            int j = idx >> 6, col = c0 + (idx & 63);
+            if (col < nb)
+                __pipeline_memcpy_async(buf + idx, V + (long long)jl[j] * nb + col, sizeof(T));
+            else
+                buf[idx] = T(0);
+        }
+        __pipeline_commit();
+    };
+    for (int Ia = blockIdx.x; Ia < a.na; Ia += gridDim.x) {
+        __syncthreads();
+        for (int idx = tid; idx < K * MP; idx += kMixThreads) {
+            int j = idx / MP, m = idx - j * MP;
+            long long o = (long long)j * a.na + Ia;
+            uint32_t e = a.fsA[o];
+            T v = T(0);
+            if (m < a.npair) v = a.m2[eri_index(a.fpA[o], m)];
+            else if (m == a.npair) v = a.a1A[o];
+            As[idx] = flip(v, e >> 31);
+            if (m == 0) jl[j] = (int)(e & 0x3fffffffu);
+        }
+        for (int i = tid; i < nb; i += kMixThreads) {
+            accs[i] = T(0);
+            pos[i] = 0;
+        }
+        __syncthreads();
+        stage(0, Bs);
+        for (int ci = 0; ci < nchunk; ci++) {
+            const int c0 = ci * kMixCols;
+            T *Bc = Bs + (size_t)(ci & 1) * K * kMixCols;
+            if (ci + 1 < nchunk) {
+                stage(ci + 1, Bs + (size_t)((ci + 1) & 1) * K * kMixCols);
+                __pipeline_wait_prior(1);
+            } else {
+                __pipeline_wait_prior(0);
+            }
+            __syncthreads();
+            T acc[TM][4];
+#pragma unroll
+            for (int i = 0; i < TM; i++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) acc[i][q] = T(0);
+#pragma unroll 4
+            for (int k = 0; k < K; k++) {
+                const T *br = Bc + k * kMixCols + tx;
+                T b0 = br[0], b1 = br[16], b2 = br[32], b3 = br[48];
+                const T *ar = As + k * MP + ty * TM;
+#pragma unroll
+                for (int i = 0; i < TM; i++) {
+                    T av = ar[i];
+                    acc[i][0] = fma(av, b0, acc[i][0]);
+                    acc[i][1] = fma(av, b1, acc[i][1]);
+                    acc[i][2] = fma(av, b2, acc[i][2]);
+                    acc[i][3] = fma(av, b3, acc[i][3]);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < TM; i++) {
+                int m = ty * TM + i;
+                if (m < a.mrows) {
+                    T *dst = Ts + (size_t)m * kMixCols + tx;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) dst[16 * q] = acc[i][q];
+                }
+            }
+            __syncthreads();
+            const int c1 = c0 + kMixCols;
+            for (int Ib = tid; Ib < nb; Ib += kMixThreads) {
+                T x = accs[Ib];
+                int p = pos[Ib];
+                const uint32_t *lst = a.sortB + (size_t)Ib * a.sb;
+                while (p < a.sb) {
+                    uint32_t e = lst[p];
+                    int J = (int)(e & 0xffffu);
+                    if (J >= c1) break;
+                    x += flip(Ts[(size_t)((e >> 16) & 0x7fffu) * kMixCols + (J - c0)], e >> 31);
+                    p++;
+                }
+                if (Ib >= c0 && Ib < c1) {
+                    const int col = Ib - c0;
+                    x += Ts[(size_t)a.npair * kMixCols + col];
+                    uint64_t oc = a.occB[Ib];
+                    while (oc) {
+                        int m = __ffsll((long long)oc);
+                        oc &= oc - 1;
+                        x += Ts[(size_t)(m * (m + 1) / 2 - 1) * kMixCols + col];
+                    }
+                }
+                accs[Ib] = x;
+                pos[Ib] = (unsigned char)p;
+            }
+            __syncthreads();
+        }
+        T *srow = S + (long long)Ia * nb;
+        for (int Ib = tid; Ib < nb; Ib += kMixThreads) srow[Ib] += accs[Ib];
+    }
+}
+
+static size_t mix2_smem(int K, int TM, int mrows, int nb, size_t w) {
+    return (size_t)K * 16 * TM * w + 2 * (size_t)K * kMixCols * w + (size_t)mrows * kMixCols * w +
+           (size_t)nb * w + (size_t)K * 4 + (size_t)nb + 64;
+}
+
+// ---- row kernel of the dense-product plan ---------------------------------
+//
+// RB consecutive alpha strings per CTA: the diagonal, the beta singles and
+// beta doubles inside each row (gathered from the RB rows staged in shared
+// memory, so one load of a beta excitation entry serves RB rows) and the
+// alpha doubles (rows streamed from global memory).  The alpha singles are
+// added by k_sigma_mixed afterwards.
+
+template <typename T, int ITEMS, int RB>
+__global__ void __launch_bounds__(ITEMS * RB <= 4 ? 1024 : 512)
+    k_sigma_rows(FciArgs<T> a, const T *__restrict__ V, T *__restrict__ S) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *rows = reinterpret_cast<T *>(smem_raw);   // RB x nb
+    T *jrow = rows + (size_t)RB * a.nb;          // RB x npair
+    const int nb = a.nb, tid = threadIdx.x, nt = blockDim.x;
+    const int Ia0 = blockIdx.x * RB;
+    const int nr = min(RB, a.na - Ia0);
+    for (int r = 0; r < nr; r++) {
+        const T *crow = V + (long long)(Ia0 + r) * nb;
+        for (int i = tid; i < nb; i += nt) rows[(size_t)r * nb + i] = crow[i];
+        for (int p = tid; p < a.npair; p += nt)
+            jrow[(size_t)r * a.npair + p] = a.jA[(long long)p * a.na + Ia0 + r];
+    }
+    __syncthreads();
+    T acc[ITEMS][RB];
+#pragma unroll
+    for (int it = 0; it < ITEMS; it++) {
+        int Ib = tid + it * nt;
+#pragma unroll
+        for (int r = 0; r < RB; r++) acc[it][r] = T(0);
+        if (Ib >= nb) continue;
+#pragma unroll
+        for (int r = 0; r < RB; r++)
+            if (r < nr) acc[it][r] = a.hd[(long long)(Ia0 + r) * nb + Ib] * rows[(size_t)r * nb + Ib];
+        for (int f = 0; f < a.sb; f++) {
+            long long o = (long long)f * nb + Ib;
+            uint32_t e = a.fsB[o];
+            T h = a.a1B[o];
+            int J = (int)(e & 0x3fffffffu), pr = a.fpB[o];
+            uint32_t neg = e >> 31;
+#pragma unroll
+            for (int r = 0; r < RB; r++)
+                acc[it][r] += flip(h + jrow[(size_t)r * a.npair + pr], neg) *
+                              rows[(size_t)r * nb + J];
+        }
+        for (int f = 0; f < a.db; f++) {
+            long long o = (long long)f * nb + Ib;
+            T h = a.dHB[o];
+            int J = a.dJB[o];
+#pragma unroll
+            for (int r = 0; r < RB; r++) acc[it][r] += h * rows[(size_t)r * nb + J];
+        }
+    }
+    // alpha doubles of each row: coefficient uniform over the CTA
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+        if (r >= nr) break;
+        for (int f = 0; f < a.da; f++) {
+            long long o = (long long)f * a.na + Ia0 + r;
+            int Ja = a.dJA[o];
+            T h = a.dHA[o];
+            const T *src = V + (long long)Ja * nb;
+#pragma unroll
+            for (int it = 0; it < ITEMS; it++) {
+                int Ib = tid + it * nt;
+                if (Ib < nb) acc[it][r] += h * src[Ib];
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+        if (r >= nr) break;
+        T *dst = S + (long long)(Ia0 + r) * nb;
+#pragma unroll
+        for (int it = 0; it < ITEMS; it++) {
+            int Ib = tid + it * nt;
+            if (Ib < nb) dst[Ib] = acc[it][r];
+        }
+    }
+}
+
+static size_t rows_smem(int nb, int npair, int RB, size_t w) {
+    return (size_t)RB * nb * w + (size_t)RB * npair * w + 16;
+}
+
 static size_t mix_smem(int K, int TM, size_t w) {
-    return (size_t)K * 16 * TM * w + (size_t)K * kMixCols * w + (size_t)K * 4 + 16;
+    return (size_t)K * 16 * TM * w + 2 * (size_t)K * kMixCols * w + (size_t)K * 4 + 16;
 }
 
 static size_t fci_smem(int nb, int npair, int R, size_t w) {
@@ -390,6 +641,23 @@ jci_status fci_prepare(jci_space *s) {
         f->smem_max = (size_t)optin;
         // the kernel needs at least the own row plus one staged row
         if (fci_smem(f->nb, f->npair, 1, sizeof(double)) > f->smem_max) f->smem_max = 0;
+        // beta singles of every string sorted by target, for k_sigma_mixed2
+        if (B.nstr < 65536 && d->npair < 32768 && B.max_sing < 256) {
+            std::vector<uint32_t> so((size_t)B.nstr * B.max_sing);
+            for (int i = 0; i < B.nstr; i++) {
+                uint32_t *row = &so[(size_t)i * B.max_sing];
+                for (int k = 0; k < B.max_sing; k++) {
+                    const Exc &x = B.sing[B.soff[i] + k];
+                    row[k] = (uint32_t)x.target | ((uint32_t)pair_index(x.io0, x.fo0) << 16) |
+                             (x.sign < 0 ? 0x80000000u : 0u);
+                }
+                std::sort(row, row + B.max_sing,
+                          [](uint32_t u, uint32_t w) { return (u & 0xffffu) < (w & 0xffffu); });
+            }
+            JCI_CUDA(cudaMalloc(&f->sortB, so.size() * sizeof(uint32_t)));
+            JCI_CUDA(cudaMemcpy(f->sortB, so.data(), so.size() * sizeof(uint32_t),
+                                cudaMemcpyHostToDevice));
+        }
     }
     for (int sp = 0; sp < 2; sp++) {
         const SpinTables &t = d->t[sp];
@@ -423,6 +691,44 @@ static jci_status launch_one(const FciArgs<T> &a, int nt, size_t smem, int na, c
     return JCI_OK;
 }
 
+template <typename T, int IT, int RB>
+static jci_status launch_rows_t(const FciArgs<T> &a, int nt, const T *v, T *o,
+                                cudaStream_t st) {
+    size_t smem = rows_smem(a.nb, a.npair, RB, sizeof(T));
+    JCI_CUDA(cudaFuncSetAttribute(k_sigma_rows<T, IT, RB>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_sigma_rows<T, IT, RB><<<(a.na + RB - 1) / RB, nt, smem, st>>>(a, v, o);
+    return JCI_OK;
+}
+
+// Row kernel of the dense-product plan with nt threads and RB rows per CTA.
+template <typename T>
+static jci_status launch_rows(const FciArgs<T> &a, int nt, int RB, const T *v, T *o,
+                              cudaStream_t st) {
+    int items = (a.nb + nt - 1) / nt;
+    int IT = items <= 2 ? 2 : items <= 4 ? 4 : items <= 8 ? 8 : items <= 16 ? 16 : 32;
+    if (items > 32 || IT * RB > 32) return JCI_ERR_ARG;
+    if (nt > (IT * RB <= 4 ? 1024 : 512)) return JCI_ERR_ARG;
+#define JCI_ROWS(I, B) \
+    if (IT == I && RB == B) return launch_rows_t<T, I, B>(a, nt, v, o, st)
+    JCI_ROWS(2, 1); JCI_ROWS(2, 2); JCI_ROWS(2, 4);
+    JCI_ROWS(4, 1); JCI_ROWS(4, 2); JCI_ROWS(4, 4);
+    JCI_ROWS(8, 1); JCI_ROWS(8, 2); JCI_ROWS(8, 4);
+    JCI_ROWS(16, 1); JCI_ROWS(16, 2);
+    JCI_ROWS(32, 1);
+#undef JCI_ROWS
+    return JCI_ERR_ARG;
+}
+
+static bool rows_ok(int nb, int nt, int RB) {
+    int items = (nb + nt - 1) / nt;
+    int IT = items <= 2 ? 2 : items <= 4 ? 4 : items <= 8 ? 8 : items <= 16 ? 16 : 32;
+    if (items > 32 || IT * RB > 32) return false;
+    if (RB != 1 && RB != 2 && RB != 4) return false;
+    if (nt != 128 && nt != 256 && nt != 512 && nt != 1024) return false;
+    return nt <= (IT * RB <= 4 ? 1024 : 512);
+}
+
 template <typename T>
 using MixKernel = void (*)(MixArgs<T>, const T *, T *, T *);
 
@@ -447,11 +753,13 @@ static bool mixed_possible(const FciTables *f, size_t w) {
     return TM <= 9 && f->sa >= 1 && mix_smem(f->sa, TM, w) <= f->smem_max;
 }
 
-// Second kernel of the dense-product path; the per-CTA scratch panels are
-// allocated on first use (grid = resident CTAs on the whole device).
+// Second kernel of the dense-product path.  The per-CTA scratch panels are
+// allocated on first use for the largest resident grid; `per_sm` picks the
+// CTAs per SM actually launched (0 = as many as fit), which trades latency
+// hiding against keeping the panels L2-resident.
 template <typename T>
 static jci_status launch_mixed(jci_space *s, const FciArgs<T> &fa, const T *v, T *o,
-                               cudaStream_t st) {
+                               cudaStream_t st, int per_sm) {
     DeviceState *d = s->dev;
     FciTables *f = d->fci;
     const int prec = sizeof(T) == 8 ? 0 : 1;
@@ -474,23 +782,86 @@ static jci_status launch_mixed(jci_space *s, const FciArgs<T> &fa, const T *v, T
         size_t bytes = (size_t)grid * m.mrows * m.nbp * sizeof(T);
         JCI_CUDA(cudaMalloc(&f->tbuf[prec], bytes));
         f->mix_grid[prec] = grid;
+        f->mix_occ[prec] = std::max(occ, 1);
+        f->nsm = nsm;
     }
-    kern<<<f->mix_grid[prec], kMixThreads, smem, st>>>(m, v, o, (T *)f->tbuf[prec]);
+    int grid = f->mix_grid[prec];
+    if (per_sm > 0 && per_sm < f->mix_occ[prec])
+        grid = std::max(1, std::min(grid, f->nsm * per_sm));
+    kern<<<grid, kMixThreads, smem, st>>>(m, v, o, (T *)f->tbuf[prec]);
+    return JCI_OK;
+}
+
+template <typename T>
+using Mix2Kernel = void (*)(Mix2Args<T>, const T *, T *);
+
+template <typename T>
+static Mix2Kernel<T> mixed2_kernel(int TM) {
+    switch (TM) {
+        case 1: return k_sigma_mixed2<T, 1>;
+        case 2: return k_sigma_mixed2<T, 2>;
+        case 3: return k_sigma_mixed2<T, 3>;
+        case 4: return k_sigma_mixed2<T, 4>;
+        case 5: return k_sigma_mixed2<T, 5>;
+        case 6: return k_sigma_mixed2<T, 6>;
+        case 7: return k_sigma_mixed2<T, 7>;
+        case 8: return k_sigma_mixed2<T, 8>;
+        case 9: return k_sigma_mixed2<T, 9>;
+        default: return nullptr;
+    }
+}
+
+static bool mixed2_possible(const FciTables *f, size_t w) {
+    int mrows = f->npair + 1, TM = (mrows + 15) / 16;
+    return f->sortB && TM <= 9 && f->sa >= 1 &&
+           mix2_smem(f->sa, TM, mrows, f->nb, w) <= f->smem_max;
+}
+
+// Panel-free product kernel with per_sm CTAs per SM (0 = as many as fit).
+template <typename T>
+static jci_status launch_mixed2(jci_space *s, const FciArgs<T> &fa, const T *v, T *o,
+                                cudaStream_t st, int per_sm) {
+    DeviceState *d = s->dev;
+    FciTables *f = d->fci;
+    Mix2Args<T> m;
+    m.na = fa.na; m.nb = fa.nb; m.nbp = (fa.nb + kMixCols - 1) / kMixCols * kMixCols;
+    m.sa = fa.sa; m.sb = fa.sb; m.npair = fa.npair; m.mrows = fa.npair + 1;
+    m.fsA = fa.fsA; m.fpA = fa.fpA; m.sortB = f->sortB;
+    m.a1A = fa.a1A; m.m2 = fa.m2; m.occB = d->t[1].occ;
+    int TM = (m.mrows + 15) / 16;
+    Mix2Kernel<T> kern = mixed2_kernel<T>(TM);
+    if (!kern || !f->sortB) return JCI_ERR_SPACE;
+    size_t smem = mix2_smem(m.sa, TM, m.mrows, m.nb, sizeof(T));
+    JCI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0, nsm = 0;
+    JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kMixThreads, smem));
+    JCI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d->device));
+    occ = std::max(occ, 1);
+    if (per_sm > 0) occ = std::min(occ, per_sm);
+    int grid = std::max(1, std::min(m.na, nsm * occ));
+    kern<<<grid, kMixThreads, smem, st>>>(m, v, o);
     return JCI_OK;
 }
 
 // One full sigma of one vector with the given plan.
+// mode 0: k_sigma_fci with R staged alpha rows.  mode 1: k_sigma_rows (nt
+// threads, B rows per CTA) then k_sigma_mixed with R CTAs per SM.
 template <typename T>
-static jci_status run_plan(jci_space *s, FciArgs<T> a, int mode, int nt, int R, const T *v, T *o,
-                           cudaStream_t st) {
+static jci_status run_plan(jci_space *s, FciArgs<T> a, int mode, int nt, int R, int B,
+                           const T *v, T *o, cudaStream_t st) {
     FciTables *f = s->dev->fci;
     size_t w = sizeof(T);
-    a.do_as = mode == 0;
-    a.R = mode == 0 ? R : 0;
-    jci_status r = launch_one<T>(a, nt, fci_smem(f->nb, f->npair, a.R, w), f->na, v, o, st);
-    if (r) return r;
-    if (mode == 1) return launch_mixed<T>(s, a, v, o, st);
-    return JCI_OK;
+    jci_status r;
+    if (mode == 0) {
+        a.do_as = 1;
+        a.R = R;
+        return launch_one<T>(a, nt, fci_smem(f->nb, f->npair, R, w), f->na, v, o, st);
+    }
+    a.do_as = 0;
+    a.R = 0;
+    if ((r = launch_rows<T>(a, nt, B, v, o, st))) return r;
+    if (mode == 2) return launch_mixed2<T>(s, a, v, o, st, R);
+    return launch_mixed<T>(s, a, v, o, st, R);
 }
 
 // Pick the plan for this space by timing the admissible candidates on
@@ -508,59 +879,93 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     JCI_CUDA(cudaMalloc(&v, n * w));
     JCI_CUDA(cudaMalloc(&o, n * w));
     JCI_CUDA(cudaMemsetAsync(v, 0, n * w, st));
-    float best = 1e30f;
-    int bnt = 0, bR = 0, bmode = 0;
     const int nts[] = {128, 256, 512, 1024};
     const int Rs[] = {1, 2, 4, 8, 16};
     cudaEvent_t e0, e1;
     JCI_CUDA(cudaEventCreate(&e0));
     JCI_CUDA(cudaEventCreate(&e1));
-    for (int mode = 0; mode < 2; mode++) {
-        if (mode == 1 && !mixed_possible(f, w)) continue;
+    jci_status err = JCI_OK;
+    // ms per call of fn (one untimed call, then two timed)
+    auto timeit = [&](auto fn) -> float {
+        if (err || (err = fn())) return 1e30f;
+        cudaEventRecord(e0, st);
+        for (int k = 0; k < 2 && !err; k++) err = fn();
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return err ? 1e30f : ms / 2;
+    };
+    auto useful = [&](int nt) {
+        int items = (f->nb + nt - 1) / nt;
+        return !(nt > 32 * ((f->nb + 31) / 32) && nt > 128) && items <= 32;  // idle threads
+    };
+    // mode 0: one kernel, R staged rows
+    float best0 = 1e30f;
+    int b0nt = 0, b0R = 0;
+    for (int nt : nts) {
+        int items = (f->nb + nt - 1) / nt;
+        if (!useful(nt) || (nt == 1024 && items > 2)) continue;
+        for (int R : Rs) {
+            if (R > f->sa && R > 1) continue;
+            if (fci_smem(f->nb, f->npair, R, w) > f->smem_max) continue;
+            float ms = timeit([&] { return run_plan<T>(s, a, 0, nt, R, 1, v, o, st); });
+            if (ms < best0) { best0 = ms; b0nt = nt; b0R = R; }
+        }
+    }
+    // mode 1: the two kernels are independent launches, tuned separately
+    float best1 = 1e30f;
+    int b1nt = 0, b1B = 0, b1R = 0, b1mode = 1;
+    if (mixed_possible(f, w)) {
+        float brow = 1e30f, bmix = 1e30f;
+        FciArgs<T> ar = a;
+        ar.do_as = 0;
+        ar.R = 0;
         for (int nt : nts) {
-            int items = (f->nb + nt - 1) / nt;
-            if (items > 32 || (nt == 1024 && items > 2)) continue;
-            if (nt > 32 * ((f->nb + 31) / 32) && nt > 128) continue;  // idle threads
-            for (int R : Rs) {
-                if (mode == 1 && R != 1) continue;
-                if (mode == 0 && R > f->sa && R > 1) continue;
-                if (fci_smem(f->nb, f->npair, mode == 0 ? R : 0, w) > f->smem_max) continue;
-                jci_status r = run_plan<T>(s, a, mode, nt, R, v, o, st);
-                if (r) return r;
-                JCI_CUDA(cudaEventRecord(e0, st));
-                for (int k = 0; k < 2; k++)
-                    if ((r = run_plan<T>(s, a, mode, nt, R, v, o, st))) return r;
-                JCI_CUDA(cudaEventRecord(e1, st));
-                JCI_CUDA(cudaEventSynchronize(e1));
-                float ms = 0.f;
-                JCI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-                if (ms < best) {
-                    best = ms;
-                    bnt = nt;
-                    bR = R;
-                    bmode = mode;
-                }
+            if (!useful(nt)) continue;
+            for (int B : {1, 2, 4}) {
+                if (!rows_ok(f->nb, nt, B) || rows_smem(f->nb, f->npair, B, w) > f->smem_max)
+                    continue;
+                float ms = timeit([&] { return launch_rows<T>(ar, nt, B, v, o, st); });
+                if (ms < brow) { brow = ms; b1nt = nt; b1B = B; }
             }
         }
+        int bmode = 1;
+        for (int R : {1, 2, 4}) {
+            float ms = timeit([&] { return launch_mixed<T>(s, ar, v, o, st, R); });
+            if (ms < bmix) { bmix = ms; b1R = R; }
+        }
+        if (mixed2_possible(f, w))
+            for (int R : {1, 2}) {
+                float ms = timeit([&] { return launch_mixed2<T>(s, ar, v, o, st, R); });
+                if (ms < bmix) { bmix = ms; b1R = R; bmode = 2; }
+            }
+        if (b1nt) best1 = brow + bmix;
+        b1mode = bmode;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(v);
     cudaFree(o);
-    if (!bnt) return JCI_ERR_SPACE;
-    f->tuned_nt[prec] = bnt;
-    f->tuned_R[prec] = bR;
-    f->tuned_mode[prec] = bmode;
-    f->tuned_ms[prec] = best / 2;
+    if (err) return err;
+    if (!b0nt && !b1nt) return JCI_ERR_SPACE;
+    bool use1 = b1nt && best1 < best0;
+    f->tuned_mode[prec] = use1 ? b1mode : 0;
+    f->tuned_nt[prec] = use1 ? b1nt : b0nt;
+    f->tuned_R[prec] = use1 ? b1R : b0R;
+    f->tuned_B[prec] = use1 ? b1B : 1;
+    f->tuned_ms[prec] = use1 ? best1 : best0;
     return JCI_OK;
 }
 
-void fci_tuning(const jci_space *s, int precision, int *nt, int *R, float *ms) {
+void fci_tuning(const jci_space *s, int precision, int *mode, int *nt, int *R, int *B,
+                float *ms) {
     const FciTables *f = s->dev ? s->dev->fci : nullptr;
     int p = precision == JCI_FP32 ? 1 : 0;
+    *mode = f ? f->tuned_mode[p] : 0;
     *nt = f ? f->tuned_nt[p] : 0;
-    // rows staged per pass; 0 when the alpha singles run as the dense product
-    *R = f ? (f->tuned_mode[p] == 1 ? 0 : f->tuned_R[p]) : 0;
+    *R = f ? f->tuned_R[p] : 0;
+    *B = f ? f->tuned_B[p] : 0;
     *ms = f ? f->tuned_ms[p] : 0.f;
 }
 
@@ -595,7 +1000,8 @@ static jci_status launch_fci(jci_space *s, int nvec, const T *V, T *S, long long
     }
     for (int c = 0; c < nvec; c++) {
         jci_status r = run_plan<T>(s, a, f->tuned_mode[prec], f->tuned_nt[prec],
-                                   f->tuned_R[prec], V + c * ld, S + c * ld, st);
+                                   f->tuned_R[prec], f->tuned_B[prec], V + c * ld, S + c * ld,
+                                   st);
         if (r) return r;
     }
     JCI_CUDA(cudaGetLastError());
@@ -611,20 +1017,27 @@ jci_status fci_sigma(jci_space *s, int nvec, const void *v, void *sig, long long
 
 // Force a plan (mode 0: staged rows R, mode 1: dense product) for tests and
 // measurements; nt = threads per CTA of the row kernel.
-jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R) {
+jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, int B) {
     FciTables *f = s->dev ? s->dev->fci : nullptr;
     if (!f) return JCI_ERR_STATE;
     int p = precision == JCI_FP32 ? 1 : 0;
     size_t w = p ? sizeof(float) : sizeof(double);
-    if (mode == 1 && !mixed_possible(f, w)) return JCI_ERR_ARG;
-    int items = (f->nb + nt - 1) / nt;
-    if ((nt != 128 && nt != 256 && nt != 512 && nt != 1024) || items > 32 ||
-        (nt == 1024 && items > 2))
-        return JCI_ERR_ARG;
-    if (mode == 0 && (R < 1 || fci_smem(f->nb, f->npair, R, w) > f->smem_max)) return JCI_ERR_ARG;
+    if (mode == 1 || mode == 2) {
+        bool ok = mode == 1 ? mixed_possible(f, w) : mixed2_possible(f, w);
+        if (!ok || !rows_ok(f->nb, nt, B) || R < 0 ||
+            rows_smem(f->nb, f->npair, B, w) > f->smem_max)
+            return JCI_ERR_ARG;
+    } else {
+        int items = (f->nb + nt - 1) / nt;
+        if ((nt != 128 && nt != 256 && nt != 512 && nt != 1024) || items > 32 ||
+            (nt == 1024 && items > 2))
+            return JCI_ERR_ARG;
+        if (R < 1 || fci_smem(f->nb, f->npair, R, w) > f->smem_max) return JCI_ERR_ARG;
+    }
     f->tuned_mode[p] = mode;
     f->tuned_nt[p] = nt;
-    f->tuned_R[p] = mode == 0 ? R : 1;
+    f->tuned_R[p] = R;
+    f->tuned_B[p] = mode != 0 ? B : 1;
     f->tuned_ms[p] = 0.f;
     return JCI_OK;
 }

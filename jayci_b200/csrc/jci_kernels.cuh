@@ -13,8 +13,9 @@ jci_status fci_prepare(jci_space *s);
 jci_status fci_sigma(jci_space *s, int nvec, const void *v, void *sig, long long ld,
                      int precision, cudaStream_t st);
 void fci_free(DeviceState *d);
-void fci_tuning(const jci_space *s, int precision, int *nt, int *R, float *ms);
-jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R);
+void fci_tuning(const jci_space *s, int precision, int *mode, int *nt, int *R, int *B,
+                float *ms);
+jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, int B);
 jci_status fci_sigma_noalloc(jci_space *s, const void *v, void *o, int precision,
                              cudaStream_t st);
 size_t fci_noalloc_scratch_bytes();

@@ -78,18 +78,20 @@ def test_sigma_against_oracle(gen):
 
 
 @pytest.mark.parametrize("name", ["cas6_6", "cas7_7", "cas10_10"])
-@pytest.mark.parametrize("plan", [(0, 128, 1), (0, 256, 4), (0, 512, 16), (1, 128, 1),
-                                  (1, 256, 1), (1, 1024, 1)])
+@pytest.mark.parametrize("plan", [(0, 128, 1, 1), (0, 256, 4, 1), (0, 512, 16, 1),
+                                  (1, 128, 1, 1), (1, 256, 2, 2), (1, 128, 0, 4),
+                                  (1, 1024, 4, 1), (1, 512, 1, 4), (2, 256, 1, 2),
+                                  (2, 512, 2, 1), (2, 128, 0, 4)])
 @pytest.mark.parametrize("prec", [jb.FP64, jb.FP32])
 def test_every_fci_plan(name, plan, prec):
     """Each launch plan the autotuner may pick gives the reference's sigma."""
     g = load(name)
     s = space_for(g)
-    mode, nt, R = plan
-    nb = g["istr1"].shape[0]
-    if (nb + nt - 1) // nt > 32 or (nt == 1024 and (nb + nt - 1) // nt > 2):
+    mode, nt, R, B = plan
+    try:
+        s.set_sigma_plan(prec, mode, nt, R, B)
+    except jb.JciError:
         pytest.skip("plan not admissible for this size")
-    s.set_sigma_plan(prec, mode, nt, R)
     S = s.sigma(g["sigma_v"], prec)
     ref = g["sigma"]
     tol = 1e-12 if prec == jb.FP64 else 2e-6
