@@ -14,8 +14,8 @@ e2e    = the same through the public C ABI (jci_sigma) from pinned host
          buffers, host->device copy of the 3 input vectors and device->host
          copy of the 3 sigma vectors inside every timed step
 Extra fields report the FP32 sigma rate and full Davidson solves (plain
-FP64 reference schedule vs mixed FP32->FP64 block Davidson, energies
-compared) measured outside the timed region.
+FP64 reference schedule vs the mixed FP32->FP64 two-phase schedule,
+energies compared) measured outside the timed region.
 
 --impl reference times the reference's own CPU code (oracle/_ref, the
 reference's mpi_source compiled unchanged against a single-process GA/MPI
@@ -45,6 +45,9 @@ WORKLOADS = {
     "fci14_14_fc2": ((18, 16, 2), 4, 49, 441),
     "fci16_16": ((16, 16, 0), 1, 64, 784),
 }
+# &dalginfo per workload: krymin, krymax, refdim, maxiter (restol 1e-8)
+DALGINFO = {"cas10_10": (4, 12, 8, 500), "fci12_12": (6, 24, 12, 500),
+            "fci14_14_fc2": (8, 24, 16, 2000), "fci16_16": (4, 12, 8, 500)}
 METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"] \
     if os.path.exists(os.path.join(ROOT, "BASELINE.json")) else "sigma-build Gdet/s"
 
@@ -73,45 +76,50 @@ def committed_traffic(workload):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock and throttle-reason sampling during the timed region: NVML
+    (the library nvidia-smi reads) polled from a thread every 2 ms, so short
+    timed regions still get samples.  Read-only: no setting is changed."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40,
+               "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
     def __init__(self, dev):
         self.dev = dev
-        self.p = None
+        self.samples, self.mask, self.mx = [], 0, None
+        self.t = None
+        self.stop_flag = False
 
     def start(self):
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "100"],
-                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            import threading
+
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.dev)
+            self.mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+
+            def run():
+                while not self.stop_flag:
+                    try:
+                        self.samples.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                        self.mask |= nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    except Exception:
+                        pass
+                    time.sleep(0.002)
+            self.t = threading.Thread(target=run, daemon=True)
+            self.t.start()
         except Exception:
-            self.p = None
+            self.t = None
 
     def stop(self):
-        if not self.p:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.p.terminate()
-        out, _ = self.p.communicate(timeout=10)
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.strip().splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self.t is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        self.stop_flag = True
+        self.t.join(timeout=5)
+        reasons = [n for n, b in self.REASONS.items() if self.mask & b]
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.mx, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
 
 
 def cpu_sample_plan(ndets, chunks=8, frac=0.25):
@@ -297,11 +305,17 @@ def run_gpu(a):
     # full solves (outside the timed region): reference schedule FP64 vs mixed block
     solves = {}
     if not a.no_solves:
-        kw = dict(maxiter=2000, krymin=6, krymax=24, nroots=nroots, refdim=12, restol=1e-8)
+        kmin, kmax, refdim, maxiter = DALGINFO[a.workload]
+        kw = dict(maxiter=maxiter, krymin=kmin, krymax=kmax, nroots=nroots, refdim=refdim,
+                  restol=1e-8)
         r64 = sp.davidson(**kw)
-        rmx = sp.davidson(precision=jb.MIXED, block=True, **kw)
+        rmx = sp.davidson(precision=jb.MIXED, **kw)
         solves = {"fp64_solve_s": r64.stats.total_seconds, "fp64_converged": r64.converged,
                   "mixed_solve_s": rmx.stats.total_seconds, "mixed_converged": rmx.converged,
+                  "fp64_sigma_vectors": r64.stats.sigma_vectors,
+                  "mixed_sigma_vectors": [rmx.stats.fp32_sigma_vectors,
+                                          rmx.stats.sigma_vectors - rmx.stats.fp32_sigma_vectors],
+                  "davidson": dict(krymin=kmin, krymax=kmax, refdim=refdim, maxiter=maxiter),
                   "fp64_solves_per_s": world / r64.stats.total_seconds,
                   "mixed_solves_per_s": world / rmx.stats.total_seconds,
                   "mixed_vs_fp64_max_abs_dE": float(np.abs(rmx.energies - r64.energies).max()),
@@ -344,6 +358,187 @@ def run_gpu(a):
     return 0
 
 
+def run_serve(a):
+    """Serving stream: CAS(m,m) solves, m uniform in {6, 8, 10, 12}, 1-4 roots,
+    chained in 32-step geometry scans (base integrals seed 105 + scan, each
+    step adds N(0, 1e-3) perturbations, seed 105000 + request), each step
+    warm-started from the previous one of its scan.  Three arms:
+      plain    -- each request solved alone through the single-solve API
+                  (FP64, reference Davidson schedule, cold start; string
+                  spaces built once per size), on the first --serve-sample
+                  steps of every scan;
+      one_slot -- the server with one slot: requests back to back, warm
+                  starts, cached spaces, the chosen precision;
+      batched  -- the server with --slots slots, Poisson arrivals at 1.5x
+                  the one_slot rate."""
+    import numpy as np
+
+    import jayci_b200 as jb
+    from jayci_b200.synth import make_integrals, perturb
+
+    rng = np.random.default_rng(105)
+    nscan = max(1, a.serve // 32)
+    sizes = rng.choice([6, 8, 10, 12], size=nscan)
+    scans = []
+    for sc in range(nscan):
+        m = int(sizes[sc])
+        ints = make_integrals(m, m, 105 + sc)
+        steps = []
+        for st in range(32):
+            if st:
+                ints = perturb(ints, 105000 + sc * 32 + st)
+            m1, m2 = ints.packed()
+            steps.append(dict(scan=sc, step=st, m=m, nroots=int(rng.integers(1, 5)),
+                              m1=m1, m2=m2, e_nuc=ints.e_nuc))
+        scans.append(steps)
+    # arrival order: a random interleaving that keeps each scan's step order
+    pos = [0] * nscan
+    seq = []
+    while len(seq) < nscan * 32:
+        sc = int(rng.choice([s for s in range(nscan) if pos[s] < 32]))
+        seq.append(scans[sc][pos[sc]])
+        pos[sc] += 1
+    N = len(seq)
+    prec = jb.MIXED if a.serve_mixed else jb.FP64
+    kw = dict(krymin=4, krymax=16, refdim=8, restol=1e-8, maxiter=2000, precision=prec)
+
+    def submit(srv, r, warm):
+        return srv.submit((r["m"], r["m"], 0, 0, r["m"], 0, 0), r["m1"], r["m2"], r["e_nuc"],
+                          0.0, nroots=r["nroots"], warm_from=warm, **kw)
+
+    def by_size(rows):
+        out = {}
+        for m in sorted(set(x[0] for x in rows)):
+            sel = [x for x in rows if x[0] == m]
+            out[f"cas{m}"] = dict(n=len(sel),
+                                  solve_ms=float(np.mean([x[1] for x in sel]) * 1e3),
+                                  iterations=float(np.mean([x[2] for x in sel])),
+                                  sigma_ms=float(np.mean([x[3] for x in sel]) * 1e3))
+        return out
+
+    # warm-up: one solve per size class (autotuning, table build)
+    srv = jb.Server(slots=1)
+    for m in sorted(set(int(x) for x in sizes)):
+        r = next(x for x in seq if x["m"] == m)
+        srv.wait(submit(srv, r, -1))
+    srv.close()
+
+    # plain single solves on a bounded sample of scan steps
+    spaces = {}
+    sample = [x for x in seq if x["step"] < a.serve_sample]
+    rows = []
+    t0 = time.perf_counter()
+    for r in sample:
+        m = r["m"]
+        if m not in spaces:
+            spaces[m] = jb.Space(m, m)
+        sp = spaces[m]
+        ts = time.perf_counter()
+        sp.set_integrals(r["m1"], r["m2"], r["e_nuc"], 0.0)
+        res = sp.davidson(maxiter=2000, krymin=4, krymax=16, nroots=r["nroots"], refdim=8,
+                          restol=1e-8, want_vectors=False)
+        rows.append((m, time.perf_counter() - ts, res.stats.iterations,
+                     res.stats.sigma_seconds))
+    t1 = time.perf_counter()
+    for sp in spaces.values():
+        sp.close()
+    plain = dict(solves_per_s=len(sample) / (t1 - t0), requests=len(sample),
+                 sample=f"steps < {a.serve_sample} of every scan",
+                 p50_ms=float(np.percentile([x[1] for x in rows], 50) * 1e3),
+                 p99_ms=float(np.percentile([x[1] for x in rows], 99) * 1e3),
+                 by_size=by_size(rows))
+
+    def play(slots, rate):
+        srv = jb.Server(slots=slots)
+        last = {}
+        tickets = []
+        t0 = time.perf_counter()
+        t_next = t0
+        arr = np.random.default_rng(7)
+        for r in seq:
+            if rate:
+                t_next += arr.exponential(1.0 / rate)
+                d = t_next - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+            t = submit(srv, r, last.get(r["scan"], -1))
+            last[r["scan"]] = t
+            tickets.append(t)
+            if not rate:
+                srv.wait(t)
+        res = [srv.wait(t) for t in tickets]
+        t1 = time.perf_counter()
+        srv.close()
+        lat = np.array([x.queue_seconds + x.solve_seconds for x in res])
+        ok = all(x.status == 0 and x.converged for x in res)
+        rows = [(r["m"], x.solve_seconds, x.iterations, x.sigma_seconds)
+                for r, x in zip(seq, res)]
+        return dict(solves_per_s=N / (t1 - t0), wall_s=t1 - t0,
+                    p50_ms=float(np.percentile(lat, 50) * 1e3),
+                    p99_ms=float(np.percentile(lat, 99) * 1e3),
+                    warm_started=int(sum(x.warm_started for x in res)), all_converged=ok,
+                    by_size=by_size(rows))
+
+    one = play(1, 0.0)
+    rate = 1.5 * one["solves_per_s"]
+    batched = play(a.slots, rate)
+    out = {"metric": "served CI solves/s (CAS(6-12) geometry-scan stream)",
+           "value": batched["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+           "requests": N, "higher_is_better": True,
+           "dtype": "f64" if not a.serve_mixed else "mixed fp32->f64",
+           "data": "synthetic (seeded integrals, 32-step scans)",
+           "config": {"workload": "serving stream", "sizes": [6, 8, 10, 12], "scans": nscan,
+                      "slots": a.slots, "arrival_rate_per_s": rate, "restol": 1e-8},
+           "plain": plain, "one_slot": one, "batched": batched,
+           "speedup_vs_plain": batched["solves_per_s"] / plain["solves_per_s"],
+           "speedup_vs_one_slot": batched["solves_per_s"] / one["solves_per_s"]}
+    print(json.dumps(out))
+    return 0
+
+
+def run_profile(a):
+    """Small fixed workload for ncu: build the space, let the sigma autotuner
+    pick its plan outside the profiled range, then run `--steps` sigma
+    applications of one vector inside the NVTX range "profile" (capture with
+    ncu --nvtx --nvtx-include "profile/")."""
+    import torch
+
+    import jayci_b200 as jb
+    from jayci_b200.synth import workload_integrals
+
+    (geo, _, _, _) = WORKLOADS[a.workload]
+    ints = workload_integrals(a.workload)
+    m1, m2 = ints.packed()
+    sp = jb.Space(*geo)
+    sp.set_integrals(m1, m2, ints.e_nuc, ints.e_fc)
+    prec = jb.FP32 if a.profile_fp32 else jb.FP64
+    st = torch.cuda.Stream()
+    dt = torch.float32 if a.profile_fp32 else torch.float64
+    with torch.cuda.stream(st):
+        v = torch.randn(sp.ndets, dtype=dt, device="cuda")
+        o = torch.empty_like(v)
+        sp.sigma_device(v.data_ptr(), o.data_ptr(), 1, sp.ndets, prec, st.cuda_stream)
+        torch.cuda.synchronize()
+        if a.profile_davidson:
+            # a few Davidson iterations: subspace products (k_gram), residuals,
+            # preconditioner and sigma as they run inside a solve
+            kmin, kmax, refdim, _ = DALGINFO[a.workload]
+            torch.cuda.nvtx.range_push("profile")
+            sp.davidson(maxiter=a.steps, krymin=kmin, krymax=kmax, nroots=1, refdim=refdim,
+                        restol=1e-8, want_vectors=False)
+            torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
+        else:
+            torch.cuda.nvtx.range_push("profile")
+            for _ in range(a.steps):
+                sp.sigma_device(v.data_ptr(), o.data_ptr(), 1, sp.ndets, prec, st.cuda_stream)
+            torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile": a.workload, "ndets": sp.ndets,
+                      "plan": sp.sigma_tuning(prec)}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -357,9 +552,24 @@ def main():
                     help="fraction of rows in the CPU-baseline sample (about 10 s)")
     ap.add_argument("--ref-step-frac", type=float, default=0.02,
                     help="fraction of rows per step of --impl reference")
+    ap.add_argument("--serve", type=int, default=0,
+                    help="run the serving stream with this many requests instead")
+    ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--serve-mixed", action="store_true")
+    ap.add_argument("--serve-sample", type=int, default=2,
+                    help="scan steps per scan solved by the plain arm")
+    ap.add_argument("--profile", action="store_true",
+                    help="run --steps sigma calls in an NVTX range for ncu")
+    ap.add_argument("--profile-fp32", action="store_true")
+    ap.add_argument("--profile-davidson", action="store_true",
+                    help="with --profile: --steps Davidson iterations instead of sigma calls")
     a = ap.parse_args()
+    if a.profile:
+        return run_profile(a)
     if a.warmup < 3:
         a.warmup = 3
+    if a.serve:
+        return run_serve(a)
     if a.impl == "reference":
         return run_reference(a)
     return run_gpu(a)

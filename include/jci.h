@@ -248,6 +248,69 @@ jci_status jci_davidson(jci_space *s, const jci_davidson_opts *o,
                         jci_davidson_stats *stats);
 
 /* ---------------------------------------------------------------------
+ * Serving: many CI solves of uneven size on one GPU with continuous
+ * batching.  Worker slots take queued requests as soon as a slot and HBM
+ * budget are free; solves in different slots run concurrently on their own
+ * streams, so their kernels overlap on the device.  String spaces (device
+ * tables and tuned sigma plans) are cached by their &general values and
+ * reused for later requests on the same space (geometry scans).  No
+ * counterpart in the reference (one solve per pjayci run).
+ * --------------------------------------------------------------------- */
+#define JCI_MAX_ROOTS 16
+
+typedef struct jci_server jci_server;
+
+typedef struct {
+        int electrons, orbitals, nfrozen, ndocc, nactive, nfrzvirt, xlevel;
+        const double *moints1; /* copied by jci_server_submit */
+        const double *moints2;
+        double nucrep, frzcore;
+        int nroots, krymin, krymax, maxiter, refdim;
+        double restol;
+        int precision;         /* JCI_FP64 or JCI_MIXED */
+        double switch_tol;
+        int block;             /* 1 = block Davidson */
+        long long warm_from;   /* ticket of an earlier, unreleased request on
+                                * the same space whose Ritz vectors start
+                                * this solve (the request waits for it), or
+                                * -1 */
+} jci_request;
+
+typedef struct {
+        int status;            /* jci_status of the solve */
+        int converged;
+        int nroots;
+        double energies[JCI_MAX_ROOTS];
+        int iterations;
+        int warm_started;
+        long long ndets;
+        double queue_seconds;  /* submit -> start */
+        double solve_seconds;  /* start -> finish */
+        long long sigma_vectors;
+        double sigma_seconds;  /* device time in sigma kernels */
+} jci_result;
+
+/* hbm_budget_bytes bounds the estimated device memory of the solves running
+ * at once (0 = 80 % of free device memory); slots = solves in flight. */
+jci_status jci_server_create(size_t hbm_budget_bytes, int slots,
+                             jci_server **out);
+/* Queue a request; returns JCI_ERR_BUSY if its estimated footprint exceeds
+ * the whole budget, JCI_ERR_SPACE / JCI_ERR_ARG for invalid requests. */
+jci_status jci_server_submit(jci_server *srv, const jci_request *req,
+                             long long *ticket);
+/* Wait up to timeout_s (< 0: forever) for a result; JCI_ERR_TIMEOUT if it
+ * is not done yet. */
+jci_status jci_server_wait(jci_server *srv, long long ticket,
+                           double timeout_s, jci_result *out);
+/* Result vectors of a finished request (nroots x ndets). */
+jci_status jci_server_vectors(jci_server *srv, long long ticket,
+                              double *civec);
+/* Drop a finished request's stored vectors and result. */
+jci_status jci_server_release(jci_server *srv, long long ticket);
+/* Finish the queued and running solves, then stop the workers. */
+void jci_server_destroy(jci_server *srv);
+
+/* ---------------------------------------------------------------------
  * Input / output formats.
  * --------------------------------------------------------------------- */
 

@@ -263,6 +263,92 @@ class Space:
         return SolveResult(e, civ, st, r == 0)
 
 
+MAX_ROOTS = 16
+
+
+class Request(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int) for k in ("electrons", "orbitals", "nfrozen", "ndocc",
+                                           "nactive", "nfrzvirt", "xlevel")] + [
+        ("moints1", ctypes.c_void_p), ("moints2", ctypes.c_void_p),
+        ("nucrep", ctypes.c_double), ("frzcore", ctypes.c_double)] + [
+        (k, ctypes.c_int) for k in ("nroots", "krymin", "krymax", "maxiter", "refdim")] + [
+        ("restol", ctypes.c_double), ("precision", ctypes.c_int),
+        ("switch_tol", ctypes.c_double), ("block", ctypes.c_int),
+        ("warm_from", ctypes.c_longlong)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("converged", ctypes.c_int),
+                ("nroots", ctypes.c_int), ("energies", ctypes.c_double * MAX_ROOTS),
+                ("iterations", ctypes.c_int), ("warm_started", ctypes.c_int),
+                ("ndets", ctypes.c_longlong), ("queue_seconds", ctypes.c_double),
+                ("solve_seconds", ctypes.c_double), ("sigma_vectors", ctypes.c_longlong),
+                ("sigma_seconds", ctypes.c_double)]
+
+
+class Server:
+    """Continuous-batching CI solve server (jci_server_*): `slots` solves in
+    flight, admitted by estimated HBM footprint within `budget_bytes`."""
+
+    def __init__(self, budget_bytes=0, slots=4):
+        L = lib()
+        vp = ctypes.c_void_p
+        L.jci_server_create.argtypes = [ctypes.c_size_t, ctypes.c_int, ctypes.POINTER(vp)]
+        L.jci_server_submit.argtypes = [vp, ctypes.POINTER(Request),
+                                        ctypes.POINTER(ctypes.c_longlong)]
+        L.jci_server_wait.argtypes = [vp, ctypes.c_longlong, ctypes.c_double,
+                                      ctypes.POINTER(Result)]
+        L.jci_server_vectors.argtypes = [vp, ctypes.c_longlong, vp]
+        L.jci_server_release.argtypes = [vp, ctypes.c_longlong]
+        L.jci_server_destroy.argtypes = [vp]
+        h = vp()
+        _check(L.jci_server_create(budget_bytes, slots, ctypes.byref(h)), "server_create")
+        self.h = h
+        self._ndets = {}
+
+    def submit(self, general, moints1, moints2, nucrep=0.0, frzcore=0.0, nroots=1,
+               krymin=None, krymax=24, maxiter=1000, refdim=8, restol=1e-8,
+               precision=FP64, switch_tol=1e-4, block=True, warm_from=-1):
+        """general = (electrons, orbitals, nfrozen, ndocc, nactive, nfrzvirt, xlevel)."""
+        m1 = np.ascontiguousarray(moints1, np.float64)
+        m2 = np.ascontiguousarray(moints2, np.float64)
+        r = Request(*general, m1.ctypes.data, m2.ctypes.data, nucrep, frzcore, nroots,
+                    krymin or max(nroots, 4), krymax, maxiter, refdim, restol, precision,
+                    switch_tol, int(block), warm_from)
+        t = ctypes.c_longlong()
+        _check(lib().jci_server_submit(self.h, ctypes.byref(r), ctypes.byref(t)), "submit")
+        self._ndets[t.value] = None
+        return t.value
+
+    def wait(self, ticket, timeout=-1.0):
+        res = Result()
+        _check(lib().jci_server_wait(self.h, ticket, timeout, ctypes.byref(res)), "wait")
+        self._ndets[ticket] = res.ndets
+        return res
+
+    def vectors(self, ticket, nroots):
+        n = self._ndets.get(ticket)
+        if n is None:
+            n = self.wait(ticket).ndets
+        out = np.zeros((nroots, n))
+        _check(lib().jci_server_vectors(self.h, ticket, _p(out)), "vectors")
+        return out
+
+    def release(self, ticket):
+        _check(lib().jci_server_release(self.h, ticket), "release")
+        self._ndets.pop(ticket, None)
+
+    def close(self):
+        if getattr(self, "h", None):
+            try:
+                lib().jci_server_destroy(self.h)
+            except Exception:
+                pass
+            self.h = None
+
+    __del__ = close
+
+
 def read_namelists(path):
     g, d, u = General(), Dalginfo(), Gpuinfo()
     _check(lib().jci_read_namelists(str(path).encode(), ctypes.byref(g), ctypes.byref(d),

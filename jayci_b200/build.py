@@ -25,7 +25,7 @@ LIB = os.path.join(HERE, "libjci.so")
 EXE = os.path.join(HERE, "jci")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["jci_space.cpp", "jci_io.cpp", "jci_api.cpp", "jci_device.cu", "jci_fci.cu",
+SOURCES = ["jci_space.cpp", "jci_io.cpp", "jci_api.cpp", "jci_server.cpp", "jci_device.cu", "jci_fci.cu",
            "jci_davidson.cu"]
 
 

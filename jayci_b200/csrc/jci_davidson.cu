@@ -9,18 +9,20 @@
 //    the space reaches krymax (:4821).  The subspace matrix is V_i . C_j for
 //    i >= j (make_subspacehmat_ga :4053 read through dsyevr's upper
 //    triangle), the residual r = sum_i y_i (c_i - theta v_i) (:3802), the
-//    correction t = r / (theta - D) (:3773).  After a collapse the sigma
-//    vectors are rotated with the same Ritz coefficients instead of being
-//    recomputed (identical in exact arithmetic).
+//    correction t = r / (theta - D) (:3773).  After a collapse every sigma
+//    vector is recomputed, as in the reference.
 //  * block = 1: block Davidson over all unconverged roots (one correction
 //    per root per iteration, two Gram-Schmidt passes), so a sigma launch
 //    processes several vectors and every root converges together.
 // Precision: JCI_FP64, or JCI_MIXED = FP32 sigma (FP32 storage and
-// accumulation) until the largest residual norm drops below switch_tol,
-// then every sigma vector of the current basis is recomputed in FP64 and
-// the iterations continue in FP64.  Basis vectors, Gram-Schmidt, residuals,
-// the Hdiag preconditioner, the Rayleigh-Ritz eigensolve and the energies
-// are FP64 throughout.
+// accumulation) until the residual norms drop below switch_tol, then the
+// basis is collapsed to the krymin lowest Ritz vectors, their sigma vectors
+// are recomputed in FP64 and the iterations continue in FP64 to restol.
+// With block = 0 the mixed schedule takes every root below switch_tol
+// before switching (two root-sequential phases) and rotates sigma vectors
+// with the Ritz coefficients at a collapse instead of recomputing them.
+// Basis vectors, Gram-Schmidt, residuals, the Hdiag preconditioner, the
+// Rayleigh-Ritz eigensolve and the energies are FP64 throughout.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -42,8 +44,8 @@ struct DavidsonBuffers {
     double *r = nullptr, *t = nullptr;
     float *v32 = nullptr, *s32 = nullptr;
     int cap32 = 0;
-    double *partial = nullptr;   // kDotBlocks x kMaxKry
-    double *dots = nullptr;      // kMaxKry
+    double *partial = nullptr;   // kDotBlocks x 64 x 16 (k_gram block partials)
+    double *dots = nullptr;      // 64 x 16 (k_gram results)
     double *G = nullptr, *evec = nullptr, *eval = nullptr;
     double *coef = nullptr;      // 2 x kMaxKry x kMaxKry
 };
@@ -60,39 +62,113 @@ void davidson_free(DeviceState *d) {
 
 // ---- kernels -------------------------------------------------------------
 
-// partial[b*m + i] = sum over this block's slice of X_i . y
-__global__ void __launch_bounds__(256) k_dots(const double *__restrict__ X, int m, long long ld,
-                                              const double *__restrict__ y, long long n,
-                                              double *partial) {
-    __shared__ double red[8][kMaxKry];
-    long long chunk = (n + gridDim.x - 1) / gridDim.x;
-    long long lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
-    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int i = 0; i < m; i++) {
-        const double *x = X + i * ld;
-        double s = 0.0;
-        for (long long k = lo + threadIdx.x; k < hi; k += blockDim.x) s += x[k] * y[k];
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (lane == 0) red[warp][i] = s;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        double s = 0.0;
-        for (int w = 0; w < 8; w++) s += red[w][i];
-        partial[blockIdx.x * kMaxKry + i] = s;
-    }
+// Tall-skinny products G = X^T Y of basis panels (X: m <= 64 vectors, Y:
+// p <= 16 vectors, each n long, vector-major with leading dimension ld) on
+// the FP64 tensor cores: mma.sync m8n8k4 with A = 8 vectors of X x 4
+// consecutive elements, B = the same 4 elements of 8 vectors of Y.  Lane
+// (g = lane/4, t = lane%4) loads element k0+t of vector 8a+g (A) and 8b+g
+// (B): each load instruction reads eight full 32-byte sectors.  Warps take
+// interleaved 4-element steps of the block's slice; their 8x8 tiles are
+// summed in warp order in shared memory, the block partials in block order
+// by k_gram_finish, so the result is bitwise reproducible.
+constexpr int kGramRows = 64, kGramCols = 16;
+
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
 }
 
-// out[i] = sum_b partial[b][i] in a fixed order (bitwise reproducible).
-__global__ void k_dots_finish(const double *__restrict__ partial, int nb, int m, double *out) {
-    int i = blockIdx.x;
-    __shared__ double red[32];
+// partial[blk][i*p + j] = sum over this block's slice of X_i . Y_j
+template <int MT, int PT>
+__global__ void __launch_bounds__(256)
+    k_gram(const double *__restrict__ X, int m, const double *__restrict__ Y, int p,
+           long long ld, long long n, long long chunk, double *__restrict__ partial) {
+    __shared__ double red[MT * 8][PT * 8];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const long long lo = (long long)blockIdx.x * chunk, hi = min(n, lo + chunk);
+    const double *xr[MT], *yr[PT];
+    bool xv[MT], yv[PT];
+#pragma unroll
+    for (int a = 0; a < MT; a++) {
+        xv[a] = 8 * a + g < m;
+        xr[a] = X + (long long)(xv[a] ? 8 * a + g : 0) * ld;
+    }
+#pragma unroll
+    for (int b = 0; b < PT; b++) {
+        yv[b] = 8 * b + g < p;
+        yr[b] = Y + (long long)(yv[b] ? 8 * b + g : 0) * ld;
+    }
+    double acc[MT][PT][2];
+#pragma unroll
+    for (int a = 0; a < MT; a++)
+#pragma unroll
+        for (int b = 0; b < PT; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
+    for (long long k0 = lo + warp * 4; k0 < hi; k0 += 64) {
+        double av[2][MT], bv[2][PT];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const long long k = k0 + 32 * u + t;
+            const bool in = k < hi;
+#pragma unroll
+            for (int a = 0; a < MT; a++) av[u][a] = in && xv[a] ? xr[a][k] : 0.0;
+#pragma unroll
+            for (int b = 0; b < PT; b++) bv[u][b] = in && yv[b] ? yr[b][k] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+#pragma unroll
+            for (int a = 0; a < MT; a++)
+#pragma unroll
+                for (int b = 0; b < PT; b++) dmma_8x8x4(acc[a][b], av[u][a], bv[u][b]);
+    }
+    // accumulator layout: lane holds row g, columns 2t and 2t+1 of each tile
+    for (int w = 0; w < 8; w++) {
+        if (warp == w) {
+#pragma unroll
+            for (int a = 0; a < MT; a++)
+#pragma unroll
+                for (int b = 0; b < PT; b++)
+#pragma unroll
+                    for (int i = 0; i < 2; i++) {
+                        double &r = red[8 * a + g][8 * b + 2 * t + i];
+                        r = w ? r + acc[a][b][i] : acc[a][b][i];
+                    }
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < m * p; e += blockDim.x)
+        partial[(long long)blockIdx.x * kGramRows * kGramCols + e] = red[e / p][e % p];
+}
+
+// out[e] = sum_b partial[b][e] in a fixed order (bitwise reproducible).
+__global__ void k_gram_finish(const double *__restrict__ partial, int nb, int mp, double *out) {
+    const int e = blockIdx.x;
     double s = 0.0;
-    for (int b = threadIdx.x; b < nb; b += 32) s += partial[b * kMaxKry + i];
+    for (int b = threadIdx.x; b < nb; b += 32) s += partial[(long long)b * kGramRows * kGramCols + e];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) red[0] = s;
-    __syncwarp();
-    if (threadIdx.x == 0 && i < m) out[i] = red[0];
+    if (threadIdx.x == 0 && e < mp) out[e] = s;
+}
+
+using GramKernel = void (*)(const double *, int, const double *, int, long long, long long,
+                            long long, double *);
+
+template <int MT>
+static GramKernel gram_kernel_p(int pt) {
+    return pt == 1 ? k_gram<MT, 1> : k_gram<MT, 2>;
+}
+
+static GramKernel gram_kernel(int mt, int pt) {
+    switch (mt) {
+        case 1: return gram_kernel_p<1>(pt);
+        case 2: return gram_kernel_p<2>(pt);
+        case 3: return gram_kernel_p<3>(pt);
+        case 4: return gram_kernel_p<4>(pt);
+        case 5: return gram_kernel_p<5>(pt);
+        case 6: return gram_kernel_p<6>(pt);
+        case 7: return gram_kernel_p<7>(pt);
+        default: return gram_kernel_p<8>(pt);
+    }
 }
 
 // out[k] = sum_i a[i] X_i[k] + sum_i b[i] Y_i[k]   (coefficients on device)
@@ -289,8 +365,9 @@ static jci_status ensure_buffers(Ctx &c, int cap, bool mixed, int maxnew) {
         JCI_CUDA(cudaMalloc(&b->r, (size_t)ld * sizeof(double)));
         JCI_CUDA(cudaMalloc(&b->t, (size_t)ld * sizeof(double)));
         if (!b->partial) {
-            JCI_CUDA(cudaMalloc(&b->partial, kDotBlocks * kMaxKry * sizeof(double)));
-            JCI_CUDA(cudaMalloc(&b->dots, kMaxKry * sizeof(double)));
+            JCI_CUDA(cudaMalloc(&b->partial,
+                                (size_t)kDotBlocks * kGramRows * kGramCols * sizeof(double)));
+            JCI_CUDA(cudaMalloc(&b->dots, kGramRows * kGramCols * sizeof(double)));
             JCI_CUDA(cudaMalloc(&b->G, kMaxKry * kMaxKry * sizeof(double)));
             JCI_CUDA(cudaMalloc(&b->evec, kMaxKry * kMaxKry * sizeof(double)));
             JCI_CUDA(cudaMalloc(&b->eval, kMaxKry * sizeof(double)));
@@ -346,26 +423,43 @@ static jci_status sigma_block(Ctx &c, int i0, int m, bool fp32) {
     return JCI_OK;
 }
 
+// out[i*p + j] = X_i . Y_j on the device (i < m <= 64, j < p <= 16)
+static jci_status gram(Ctx &c, const double *X, int m, const double *Y, int p, double *out) {
+    if (m < 1 || m > kGramRows || p < 1 || p > kGramCols) return JCI_ERR_ARG;
+    long long chunk = ((c.n + kDotBlocks - 1) / kDotBlocks + 63) / 64 * 64;
+    int nb = (int)((c.n + chunk - 1) / chunk);
+    gram_kernel((m + 7) / 8, (p + 7) / 8)<<<nb, 256, 0, c.st>>>(X, m, Y, p, c.ld, c.n, chunk,
+                                                                 c.b->partial);
+    k_gram_finish<<<m * p, 32, 0, c.st>>>(c.b->partial, nb, m * p, out);
+    JCI_CUDA(cudaGetLastError());
+    return JCI_OK;
+}
+
 // dots[i] = X_i . y for i < m (device), optionally copied to host
 static jci_status dots(Ctx &c, const double *X, int m, const double *y, double *host) {
-    k_dots<<<kDotBlocks, 256, 0, c.st>>>(X, m, c.ld, y, c.n, c.b->partial);
-    k_dots_finish<<<m, 32, 0, c.st>>>(c.b->partial, kDotBlocks, m, c.b->dots);
+    jci_status r = gram(c, X, m, y, 1, c.b->dots);
+    if (r) return r;
     if (host) {
         JCI_CUDA(cudaMemcpyAsync(host, c.b->dots, m * sizeof(double), cudaMemcpyDeviceToHost,
                                  c.st));
         JCI_CUDA(cudaStreamSynchronize(c.st));
     }
-    JCI_CUDA(cudaGetLastError());
     return JCI_OK;
 }
 
-// G[i][j] = V_i . C_j for rows i in [r0, r1) and j <= i (lower triangle)
+// G[i][j] = V_i . C_j for rows i in [r0, r1) and j <= i (lower triangle):
+// one tensor-core product C[0, r1)^T V[i0, i0 + p) per 16 new rows
 static jci_status gram_rows(Ctx &c, int r0, int r1, std::vector<double> &G) {
-    std::vector<double> h(kMaxKry);
-    for (int i = r0; i < r1; i++) {
-        jci_status r = dots(c, c.b->C, i + 1, c.b->V + i * c.ld, h.data());
+    std::vector<double> h((size_t)kGramRows * kGramCols);
+    for (int i0 = r0; i0 < r1; i0 += kGramCols) {
+        int p = std::min(kGramCols, r1 - i0), m = i0 + p;
+        jci_status r = gram(c, c.b->C, m, c.b->V + i0 * c.ld, p, c.b->dots);
         if (r) return r;
-        for (int j = 0; j <= i; j++) G[i * kMaxKry + j] = h[j];
+        JCI_CUDA(cudaMemcpyAsync(h.data(), c.b->dots, (size_t)m * p * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c.st));
+        JCI_CUDA(cudaStreamSynchronize(c.st));
+        for (int i = i0; i < i0 + p; i++)
+            for (int j = 0; j <= i; j++) G[i * kMaxKry + j] = h[(size_t)j * p + (i - i0)];
     }
     return JCI_OK;
 }
@@ -376,12 +470,9 @@ static jci_status rayleigh_ritz(Ctx &c, int m, const std::vector<double> &G,
     JCI_CUDA(cudaMemcpyAsync(b->G, G.data(), kMaxKry * kMaxKry * sizeof(double),
                              cudaMemcpyHostToDevice, c.st));
     size_t smem = 2 * (size_t)m * (m + 1) * sizeof(double);
-    static bool attr_set = false;
-    if (!attr_set) {
-        JCI_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(2 * kMaxKry * (kMaxKry + 1) * sizeof(double))));
-        attr_set = true;
-    }
+    // the attribute is per device; setting it again is harmless and cheap
+    JCI_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(2 * kMaxKry * (kMaxKry + 1) * sizeof(double))));
     k_jacobi<<<1, 32, smem, c.st>>>(b->G, m, kMaxKry, b->eval, b->evec, c.d_info);
     int info = 0;
     JCI_CUDA(cudaMemcpyAsync(w.data(), b->eval, m * sizeof(double), cudaMemcpyDeviceToHost, c.st));
@@ -409,10 +500,11 @@ static jci_status lincomb(Ctx &c, double *out, const double *X, const double *a,
 }
 
 // V <- V Y^T[:, :k] (and C likewise): Ritz vectors of the first k roots
-static jci_status collapse(Ctx &c, int m, int k, const std::vector<double> &Y) {
+static jci_status collapse(Ctx &c, int m, int k, const std::vector<double> &Y,
+                           bool rotate_c = true) {
     DavidsonBuffers *b = c.b;
     jci_status r;
-    for (int pass = 0; pass < 2; pass++) {
+    for (int pass = 0; pass < (rotate_c ? 2 : 1); pass++) {
         double *src = pass ? b->C : b->V;
         for (int i = 0; i < k; i++)
             if ((r = lincomb(c, b->X + i * c.ld, src, &Y[i * kMaxKry], m, nullptr, nullptr, 0)))
@@ -423,6 +515,22 @@ static jci_status collapse(Ctx &c, int m, int k, const std::vector<double> &Y) {
                                  c.st));
     }
     return JCI_OK;
+}
+
+// Precision switch of the mixed schedule: collapse the basis to its `keep`
+// lowest Ritz vectors from the FP32 phase and recompute only their sigma
+// vectors in FP64 (the FP32 sigma vectors of the dropped directions are
+// never needed in FP64), then rebuild the subspace matrix.
+static jci_status switch_to_fp64(Ctx &c, int &ckdim, int keep, std::vector<double> &G,
+                                 std::vector<double> &w, std::vector<double> &Y) {
+    jci_status r;
+    if (keep < ckdim) {
+        if ((r = collapse(c, ckdim, keep, Y, false))) return r;
+        ckdim = keep;
+    }
+    if ((r = sigma_block(c, 0, ckdim, false))) return r;
+    if ((r = gram_rows(c, 0, ckdim, G))) return r;
+    return rayleigh_ritz(c, ckdim, G, w, Y);
 }
 
 // orthonormalise t against V_0..V_{m-1} (npass classical Gram-Schmidt
@@ -496,12 +604,25 @@ static jci_status run_sequential(Ctx &c, const jci_davidson_opts *o, bool mixed,
     std::vector<double> G(kMaxKry * kMaxKry, 0.0), yc(kMaxKry), ycv(kMaxKry);
     int kmin = o->krymin, kmax = o->krymax, nroots = o->nroots;
     bool fp32 = mixed;
+    // The reference recomputes every sigma vector after a collapse
+    // (pdavidson.c:39 loop); the mixed schedule rotates them with the Ritz
+    // coefficients instead (the same vectors in exact arithmetic).
+    const bool recompute = !mixed;
+    // Mixed: phase 1 takes every root, one after the other, below
+    // switch_tol with FP32 sigma; phase 2 collapses to the krymin lowest
+    // Ritz vectors, recomputes their sigma in FP64 and refines every root
+    // from the first to restol.
+    double tol = mixed ? o->switch_tol : o->restol;
     int croot = 1, cflag = 0;
+    bool have_sigma = false;
     ckdim = kmin;
     citer = 1;
     jci_status r;
     while (citer < o->maxiter && croot <= nroots) {
-        if ((r = sigma_block(c, 0, ckdim, fp32))) return r;
+        if (recompute || !have_sigma) {
+            if ((r = sigma_block(c, 0, ckdim, fp32))) return r;
+            have_sigma = true;
+        }
         if ((r = gram_rows(c, 0, ckdim, G))) return r;
         if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
         while (ckdim < kmax) {
@@ -518,15 +639,15 @@ static jci_status run_sequential(Ctx &c, const jci_davidson_opts *o, bool mixed,
             if (o->printlvl > 0)
                 printf("  iter %4d  root %d  E = %18.12f  ||r|| = %.3e%s\n", citer, croot,
                        th + c.s->nucrep + c.s->frzcore, rnorm, fp32 ? "  (fp32 sigma)" : "");
-            if (fp32 && rnorm < o->switch_tol) {
-                // switch: recompute every sigma vector in FP64
+            cflag = rnorm < tol ? (croot < nroots ? 1 : 2) : 0;
+            if (cflag == 2 && fp32) {
                 fp32 = false;
-                if ((r = sigma_block(c, 0, ckdim, false))) return r;
-                if ((r = gram_rows(c, 0, ckdim, G))) return r;
-                if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
+                tol = o->restol;
+                croot = 1;
+                cflag = 0;
+                if ((r = switch_to_fp64(c, ckdim, kmin, G, w, Y))) return r;
                 continue;
             }
-            cflag = rnorm < o->restol ? (croot < nroots ? 1 : 2) : 0;
             if (cflag == 2) break;
             if (cflag == 1) {
                 croot++;
@@ -543,7 +664,7 @@ static jci_status run_sequential(Ctx &c, const jci_davidson_opts *o, bool mixed,
             if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
             citer++;
         }
-        if ((r = collapse(c, ckdim, kmin, Y))) return r;
+        if ((r = collapse(c, ckdim, kmin, Y, !recompute))) return r;
         ckdim = kmin;
         if (cflag == 2) break;
     }
@@ -590,9 +711,7 @@ static jci_status run_block(Ctx &c, const jci_davidson_opts *o, bool mixed,
         }
         if (fp32 && rmax < o->switch_tol) {
             fp32 = false;
-            if ((r = sigma_block(c, 0, ckdim, false))) return r;
-            if ((r = gram_rows(c, 0, ckdim, G))) return r;
-            if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
+            if ((r = switch_to_fp64(c, ckdim, std::max(kmin, nroots), G, w, Y))) return r;
             continue;
         }
         if (rmax < o->restol) {
@@ -703,6 +822,19 @@ jci_status davidson(jci_space *s, const jci_davidson_opts *o, double *energies, 
         stats->fp32_sigma_vectors = c.fp32_vecs;
     }
     return conv ? JCI_OK : JCI_ERR_NOCONV;
+}
+
+// First k basis vectors left by the last solve on this handle (after the
+// final collapse these are the Ritz vectors of the lowest k roots).
+jci_status davidson_vectors(jci_space *s, int k, double *out) {
+    DeviceState *d = s->dev;
+    if (!d || !d->dav || k > d->dav->cap) return JCI_ERR_STATE;
+    DavidsonBuffers *b = d->dav;
+    for (int i = 0; i < k; i++)
+        JCI_CUDA(cudaMemcpyAsync(out + (size_t)i * s->ndets, b->V + i * b->ld,
+                                 s->ndets * sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+    JCI_CUDA(cudaStreamSynchronize(d->stream));
+    return JCI_OK;
 }
 
 // ---- host helpers --------------------------------------------------------

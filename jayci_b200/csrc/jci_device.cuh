@@ -17,6 +17,21 @@ namespace jci {
 
 jci_status cuda_fail(cudaError_t e, const char *what, const char *file, int line);
 
+// Raise a kernel's dynamic shared-memory cap to the device's opt-in maximum.
+// The cap is an attribute of the function in the context, shared by every
+// host thread: setting it to one launch's own size would shrink it under a
+// concurrent launch of the same kernel for a larger space (solve server).
+template <typename K>
+inline cudaError_t smem_optin(K kern) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    return e;
+}
+
 // Packed excitation entry.
 //   x: bits 0..29 target string, bit 31 set for a negative phase
 //   y (single): io | fo << 8 | pair << 16   (pair = packed index of (io,fo))

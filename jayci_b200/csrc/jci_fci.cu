@@ -602,9 +602,8 @@ static size_t fci_smem(int nb, int npair, int R, size_t w) {
 }
 
 template <typename T, int ITEMS>
-static jci_status set_smem_attr(size_t bytes) {
-    JCI_CUDA(cudaFuncSetAttribute(k_sigma_fci<T, ITEMS>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+static jci_status set_smem_attr(size_t) {
+    JCI_CUDA(smem_optin(k_sigma_fci<T, ITEMS>));
     return JCI_OK;
 }
 
@@ -695,8 +694,7 @@ template <typename T, int IT, int RB>
 static jci_status launch_rows_t(const FciArgs<T> &a, int nt, const T *v, T *o,
                                 cudaStream_t st) {
     size_t smem = rows_smem(a.nb, a.npair, RB, sizeof(T));
-    JCI_CUDA(cudaFuncSetAttribute(k_sigma_rows<T, IT, RB>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    JCI_CUDA(smem_optin(k_sigma_rows<T, IT, RB>));
     k_sigma_rows<T, IT, RB><<<(a.na + RB - 1) / RB, nt, smem, st>>>(a, v, o);
     return JCI_OK;
 }
@@ -772,9 +770,8 @@ static jci_status launch_mixed(jci_space *s, const FciArgs<T> &fa, const T *v, T
     MixKernel<T> kern = mixed_kernel<T>(TM);
     if (!kern) return JCI_ERR_SPACE;
     size_t smem = mix_smem(m.sa, TM, sizeof(T));
+    JCI_CUDA(smem_optin(kern));
     if (!f->mix_grid[prec]) {
-        JCI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
         int occ = 0, nsm = 0;
         JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kMixThreads, smem));
         JCI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d->device));
@@ -832,7 +829,7 @@ static jci_status launch_mixed2(jci_space *s, const FciArgs<T> &fa, const T *v, 
     Mix2Kernel<T> kern = mixed2_kernel<T>(TM);
     if (!kern || !f->sortB) return JCI_ERR_SPACE;
     size_t smem = mix2_smem(m.sa, TM, m.mrows, m.nb, sizeof(T));
-    JCI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    JCI_CUDA(smem_optin(kern));
     int occ = 0, nsm = 0;
     JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kMixThreads, smem));
     JCI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d->device));
@@ -1118,7 +1115,7 @@ static jci_status sigma_noalloc(jci_space *s, const T *v, T *o, cudaStream_t st)
     int nt = f->tuned_nt[prec] ? f->tuned_nt[prec] : (a.nb > 2048 ? 512 : 256);
     if ((r = launch_one<T>(a, nt, fci_smem(a.nb, a.npair, 0, w), a.na, v, o, st))) return r;
     size_t smem = mix_smem(m.sa, TM, w);
-    JCI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    JCI_CUDA(smem_optin(kern));
     int occ = 0, nsm = 0;
     JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kMixThreads, smem));
     JCI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d->device));

@@ -76,6 +76,7 @@ jci_status device_sigma(jci_space *s, int nvec, const void *v, void *sig,
 float device_last_sigma_ms(jci_space *s);
 jci_status davidson(jci_space *s, const jci_davidson_opts *o,
                     double *energies, double *civec, jci_davidson_stats *st);
+jci_status davidson_vectors(jci_space *s, int k, double *out);
 
 // I/O helpers (jci_io.cpp).
 jci_status write_vectors(const char *path, int dim, int len, const double *v);

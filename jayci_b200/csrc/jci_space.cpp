@@ -17,23 +17,24 @@
 // target group when queried).
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "jci_internal.h"
 
 namespace jci {
 
 static long long g_binom[kMaxOrb + 2][kMaxElec + 2];
-static bool g_binom_ready = false;
+static std::once_flag g_binom_once;
 
 static void init_binom() {
-    if (g_binom_ready) return;
-    for (int n = 0; n <= kMaxOrb + 1; n++)
-        for (int k = 0; k <= kMaxElec + 1; k++) {
-            if (k == 0) g_binom[n][k] = 1;
-            else if (n == 0) g_binom[n][k] = 0;
-            else g_binom[n][k] = g_binom[n - 1][k - 1] + g_binom[n - 1][k];
-        }
-    g_binom_ready = true;
+    std::call_once(g_binom_once, [] {
+        for (int n = 0; n <= kMaxOrb + 1; n++)
+            for (int k = 0; k <= kMaxElec + 1; k++) {
+                if (k == 0) g_binom[n][k] = 1;
+                else if (n == 0) g_binom[n][k] = 0;
+                else g_binom[n][k] = g_binom[n - 1][k - 1] + g_binom[n - 1][k];
+            }
+    });
 }
 
 long long binom(int n, int k) {

@@ -113,6 +113,15 @@ def test_namelist_defaults_and_errors(tmp_path):
         jb.read_namelists(tmp_path / "nope.in")
 
 
+def test_server_needs_a_device():
+    """Without a CUDA device the server refuses to start (no CPU fallback)."""
+    if jb.device_count() > 0:
+        pytest.skip("a device is present")
+    with pytest.raises(jb.JciError) as ei:
+        jb.Server(slots=2)
+    assert ei.value.status == 5
+
+
 def test_vector_files(tmp_path):
     v = np.random.default_rng(1).standard_normal((3, 17))
     p = tmp_path / "civec"
