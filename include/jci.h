@@ -224,6 +224,12 @@ typedef struct {
                            * 1 = block Davidson over all unconverged roots */
         const double *init; /* prediagr == 3: krymin start vectors, or NULL
                              * to read "ci.restart" from the cwd */
+        int host_loop;    /* 0 (default): the iterations of the
+                           * root-sequential schedule run as a captured CUDA
+                           * graph launched in batches, with the control
+                           * state on the device; 1: every kernel of every
+                           * iteration is launched from the host (same
+                           * arithmetic, same results) */
 } jci_davidson_opts;
 
 typedef struct {

@@ -50,7 +50,7 @@ class DavidsonOpts(ctypes.Structure):
                 ("restol", ctypes.c_double), ("precision", ctypes.c_int),
                 ("switch_tol", ctypes.c_double), ("printlvl", ctypes.c_int),
                 ("write_files", ctypes.c_int), ("block", ctypes.c_int),
-                ("init", ctypes.c_void_p)]
+                ("init", ctypes.c_void_p), ("host_loop", ctypes.c_int)]
 
 
 class DavidsonStats(ctypes.Structure):
@@ -243,13 +243,14 @@ class Space:
     def davidson(self, maxiter=500, krymin=4, krymax=12, nroots=1, prediagr=1,
                  refdim=8, restol=1e-8, precision=FP64, switch_tol=1e-4,
                  block=False, printlvl=0, write_files=False, init=None,
-                 want_vectors=True) -> SolveResult:
+                 want_vectors=True, host_loop=False) -> SolveResult:
         o = DavidsonOpts()
         lib().jci_davidson_defaults(ctypes.byref(o))
         o.maxiter, o.krymin, o.krymax, o.nroots = maxiter, krymin, krymax, nroots
         o.prediagr, o.refdim, o.restol = prediagr, refdim, restol
         o.precision, o.switch_tol, o.block = precision, switch_tol, int(block)
         o.printlvl, o.write_files = printlvl, int(write_files)
+        o.host_loop = int(host_loop)
         if init is not None:
             init = np.ascontiguousarray(init, np.float64)
             o.init = init.ctypes.data

@@ -36,6 +36,28 @@ namespace jci {
 
 constexpr int kMaxKry = 64;
 constexpr int kDotBlocks = 296;  // 2 x 148 SMs
+constexpr int kHist = kMaxKry + 2;
+
+// Control block of a graph-captured iteration of the root-sequential
+// schedule (device memory).  The host writes it before a batch of graph
+// launches and reads it afterwards; every kernel of the captured iteration
+// takes its sizes from it and returns at once once stop is set, so launches
+// after the stop cost a few microseconds and no sigma work.
+struct DavCtl {
+    int ckdim;     // basis vectors
+    int croot;     // current root, 0-based
+    int stop;      // 0 running, 1 residual below tol, 2 basis full, 3 eigensolve failed
+    int iters;     // vectors added since the host wrote the block
+    int nhist;     // residual tests recorded in the history
+    int pad;
+    double tol;    // residual-norm tolerance of the current phase
+    double theta;  // Ritz value of the current root
+};
+
+struct DavHist {
+    int root, ckdim;
+    double theta, rnorm;
+};
 
 struct DavidsonBuffers {
     long long ld = 0;
@@ -48,13 +70,31 @@ struct DavidsonBuffers {
     double *dots = nullptr;      // 64 x 16 (k_gram results)
     double *G = nullptr, *evec = nullptr, *eval = nullptr;
     double *coef = nullptr;      // 2 x kMaxKry x kMaxKry
+    // graph-captured iterations
+    DavCtl *ctl = nullptr;
+    DavHist *hist = nullptr;     // kHist
+    double *cnew = nullptr;      // sigma of the new basis vector (ld)
+    int *info = nullptr;         // status word of k_jacobi
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // FP64, FP32 sigma
+    int gkmax[2] = {0, 0};
+    int gplan[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
 };
+
+static void drop_graphs(DavidsonBuffers *b) {
+    for (int i = 0; i < 2; i++) {
+        if (b->gexec[i]) cudaGraphExecDestroy(b->gexec[i]);
+        b->gexec[i] = nullptr;
+        b->gkmax[i] = 0;
+    }
+}
 
 void davidson_free(DeviceState *d) {
     DavidsonBuffers *b = d->dav;
     if (!b) return;
+    drop_graphs(b);
     void *p[] = {b->V, b->C, b->X, b->Y2, b->r, b->t, b->v32, b->s32, b->partial,
-                 b->dots, b->G, b->evec, b->eval, b->coef};
+                 b->dots, b->G, b->evec, b->eval, b->coef, b->ctl, b->hist, b->cnew,
+                 b->info};
     for (void *q : p) cudaFree(q);
     delete b;
     d->dav = nullptr;
@@ -79,11 +119,22 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
+// Row count taken from a graph-captured iteration's control block: m =
+// *mdev + madd (must stay <= 8 MT); kernels return at once when *stop != 0.
+struct GramDev {
+    const int *stop = nullptr;
+    const int *mdev = nullptr;
+    int madd = 0;
+};
+
 // partial[blk][i*p + j] = sum over this block's slice of X_i . Y_j
 template <int MT, int PT>
 __global__ void __launch_bounds__(256)
     k_gram(const double *__restrict__ X, int m, const double *__restrict__ Y, int p,
-           long long ld, long long n, long long chunk, double *__restrict__ partial) {
+           long long ld, long long n, long long chunk, double *__restrict__ partial,
+           GramDev gd) {
+    if (gd.stop && *gd.stop) return;
+    if (gd.mdev) m = *gd.mdev + gd.madd;
     __shared__ double red[MT * 8][PT * 8];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const long long lo = (long long)blockIdx.x * chunk, hi = min(n, lo + chunk);
@@ -142,7 +193,10 @@ __global__ void __launch_bounds__(256)
 }
 
 // out[e] = sum_b partial[b][e] in a fixed order (bitwise reproducible).
-__global__ void k_gram_finish(const double *__restrict__ partial, int nb, int mp, double *out) {
+__global__ void k_gram_finish(const double *__restrict__ partial, int nb, int mp, double *out,
+                              GramDev gd, int p) {
+    if (gd.stop && *gd.stop) return;
+    if (gd.mdev) mp = (*gd.mdev + gd.madd) * p;
     const int e = blockIdx.x;
     double s = 0.0;
     for (int b = threadIdx.x; b < nb; b += 32) s += partial[(long long)b * kGramRows * kGramCols + e];
@@ -151,7 +205,7 @@ __global__ void k_gram_finish(const double *__restrict__ partial, int nb, int mp
 }
 
 using GramKernel = void (*)(const double *, int, const double *, int, long long, long long,
-                            long long, double *);
+                            long long, double *, GramDev);
 
 template <int MT>
 static GramKernel gram_kernel_p(int pt) {
@@ -172,9 +226,15 @@ static GramKernel gram_kernel(int mt, int pt) {
 }
 
 // out[k] = sum_i a[i] X_i[k] + sum_i b[i] Y_i[k]   (coefficients on device)
+// (with ctl: mx = my = ctl->ckdim, nothing when ctl->stop)
 __global__ void k_lincomb(double *__restrict__ out, long long n, long long ld,
                           const double *__restrict__ X, const double *__restrict__ a, int mx,
-                          const double *__restrict__ Y, const double *__restrict__ b, int my) {
+                          const double *__restrict__ Y, const double *__restrict__ b, int my,
+                          const DavCtl *ctl) {
+    if (ctl) {
+        if (ctl->stop) return;
+        mx = my = ctl->ckdim;
+    }
     __shared__ double ca[kMaxKry], cb[kMaxKry];
     for (int i = threadIdx.x; i < mx; i += blockDim.x) ca[i] = a[i];
     for (int i = threadIdx.x; i < my; i += blockDim.x) cb[i] = b[i];
@@ -191,7 +251,11 @@ __global__ void k_lincomb(double *__restrict__ out, long long n, long long ld,
 // t -= sum_i ov[i] X_i ; used by classical Gram-Schmidt
 __global__ void k_orth_update(double *__restrict__ t, long long n, long long ld,
                               const double *__restrict__ X, const double *__restrict__ ov,
-                              int m) {
+                              int m, const DavCtl *ctl) {
+    if (ctl) {
+        if (ctl->stop) return;
+        m = ctl->ckdim;
+    }
     __shared__ double c[kMaxKry];
     for (int i = threadIdx.x; i < m; i += blockDim.x) c[i] = ov[i];
     __syncthreads();
@@ -205,7 +269,12 @@ __global__ void k_orth_update(double *__restrict__ t, long long n, long long ld,
 
 // t = r / (theta - D)   (generate_newvector, pdavidson.c:3773)
 __global__ void k_precond(const double *__restrict__ r, const double *__restrict__ D,
-                          double theta, double *__restrict__ t, long long n) {
+                          double theta, double *__restrict__ t, long long n,
+                          const DavCtl *ctl) {
+    if (ctl) {
+        if (ctl->stop) return;
+        theta = ctl->theta;
+    }
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
          k += (long long)gridDim.x * blockDim.x) {
         double den = theta - D[k];
@@ -216,7 +285,9 @@ __global__ void k_precond(const double *__restrict__ r, const double *__restrict
 }
 
 // x *= 1 / sqrt(*nrm2)
-__global__ void k_normalize(double *__restrict__ x, long long n, const double *__restrict__ nrm2) {
+__global__ void k_normalize(double *__restrict__ x, long long n, const double *__restrict__ nrm2,
+                            const int *stop) {
+    if (stop && *stop) return;
     double s = 1.0 / sqrt(*nrm2);
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
          k += (long long)gridDim.x * blockDim.x)
@@ -224,7 +295,8 @@ __global__ void k_normalize(double *__restrict__ x, long long n, const double *_
 }
 
 __global__ void k_d2f(const double *__restrict__ in, float *__restrict__ out, long long n,
-                      long long ldi, long long ldo, int m) {
+                      long long ldi, long long ldo, int m, const int *stop) {
+    if (stop && *stop) return;
     for (int c = 0; c < m; c++)
         for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
              k += (long long)gridDim.x * blockDim.x)
@@ -232,7 +304,8 @@ __global__ void k_d2f(const double *__restrict__ in, float *__restrict__ out, lo
 }
 
 __global__ void k_f2d(const float *__restrict__ in, double *__restrict__ out, long long n,
-                      long long ldi, long long ldo, int m) {
+                      long long ldi, long long ldo, int m, const int *stop) {
+    if (stop && *stop) return;
     for (int c = 0; c < m; c++)
         for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
              k += (long long)gridDim.x * blockDim.x)
@@ -244,7 +317,11 @@ __global__ void k_f2d(const float *__restrict__ in, double *__restrict__ out, lo
 // w; eigenvector k in Y[k*ldg + .], sign fixed so that its largest-magnitude
 // component is positive.  info = number of sweeps, or -1 if not converged.
 __global__ void k_jacobi(const double *__restrict__ G, int m, int ldg, double *w, double *Y,
-                         int *info) {
+                         int *info, const DavCtl *ctl) {
+    if (ctl) {
+        if (ctl->stop) return;
+        m = ctl->ckdim;
+    }
     extern __shared__ double sm[];
     double *A = sm;                 // m x (m+1)
     double *Vm = sm + m * (m + 1);  // m x (m+1)
@@ -328,6 +405,60 @@ __global__ void k_jacobi(const double *__restrict__ G, int m, int ldg, double *w
     }
 }
 
+// ---- kernels of a graph-captured iteration (one CTA, except k_it_store) ----
+
+// residual coefficients of the current root: r = C y - theta V y
+__global__ void k_it_begin(DavCtl *c, const double *__restrict__ eval,
+                           const double *__restrict__ evec, double *coef) {
+    if (c->stop) return;
+    const int k = c->croot, m = c->ckdim;
+    const double th = eval[k];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        double y = evec[k * kMaxKry + i];
+        coef[i] = y;
+        coef[kMaxKry + i] = -th * y;
+    }
+    if (threadIdx.x == 0) c->theta = th;
+}
+
+// residual-norm test; the iteration is recorded for the host's log
+__global__ void k_it_check(DavCtl *c, const double *__restrict__ rn2, DavHist *hist) {
+    if (c->stop) return;
+    const double rn = sqrt(*rn2);
+    const int h = c->nhist;
+    if (h < kHist) hist[h] = DavHist{c->croot, c->ckdim, c->theta, rn};
+    c->nhist = h + 1;
+    if (rn < c->tol) c->stop = 1;
+}
+
+// dst + (ckdim + off) * ld  <-  src
+__global__ void k_it_store(double *__restrict__ dst, long long ld, int off,
+                           const double *__restrict__ src, long long n, const DavCtl *c) {
+    if (c->stop) return;
+    double *d = dst + (long long)(c->ckdim + off) * ld;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x)
+        d[k] = src[k];
+}
+
+// new row G[ckdim][0..ckdim] of the subspace matrix; the basis grows by one
+__global__ void k_it_append(DavCtl *c, const double *__restrict__ dots, double *G) {
+    if (c->stop) return;
+    const int m = c->ckdim;
+    for (int j = threadIdx.x; j <= m; j += blockDim.x) G[m * kMaxKry + j] = dots[j];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        c->ckdim = m + 1;
+        c->iters++;
+    }
+}
+
+__global__ void k_it_end(DavCtl *c, const int *__restrict__ info, int kmax) {
+    if (c->stop) return;
+    if (*info < 0) c->stop = 3;
+    else if (c->ckdim >= kmax) c->stop = 2;
+}
+
 // ---- host driver ---------------------------------------------------------
 
 static unsigned grid_for(long long n) {
@@ -343,6 +474,7 @@ struct Ctx {
     long long n, ld;
     int *d_info = nullptr;
     double sigma_ms = 0.0;
+    double ms_per_vec[2] = {0.0, 0.0};  // last measured sigma time per vector (FP64, FP32)
     int sigma_calls = 0;
     long long sigma_vecs = 0;
     int fp32_vecs = 0;
@@ -355,7 +487,8 @@ static jci_status ensure_buffers(Ctx &c, int cap, bool mixed, int maxnew) {
     c.b = b;
     long long ld = (c.n + 31) / 32 * 32;
     if (b->ld != ld || b->cap < cap) {
-        void *p[] = {b->V, b->C, b->X, b->r, b->t};
+        drop_graphs(b);
+        void *p[] = {b->V, b->C, b->X, b->r, b->t, b->cnew};
         for (void *q : p) cudaFree(q);
         b->ld = ld;
         b->cap = cap;
@@ -364,7 +497,11 @@ static jci_status ensure_buffers(Ctx &c, int cap, bool mixed, int maxnew) {
         JCI_CUDA(cudaMalloc(&b->X, (size_t)cap * ld * sizeof(double)));
         JCI_CUDA(cudaMalloc(&b->r, (size_t)ld * sizeof(double)));
         JCI_CUDA(cudaMalloc(&b->t, (size_t)ld * sizeof(double)));
+        JCI_CUDA(cudaMalloc(&b->cnew, (size_t)ld * sizeof(double)));
         if (!b->partial) {
+            JCI_CUDA(cudaMalloc(&b->ctl, sizeof(DavCtl)));
+            JCI_CUDA(cudaMalloc(&b->hist, kHist * sizeof(DavHist)));
+            JCI_CUDA(cudaMalloc(&b->info, sizeof(int)));
             JCI_CUDA(cudaMalloc(&b->partial,
                                 (size_t)kDotBlocks * kGramRows * kGramCols * sizeof(double)));
             JCI_CUDA(cudaMalloc(&b->dots, kGramRows * kGramCols * sizeof(double)));
@@ -375,6 +512,7 @@ static jci_status ensure_buffers(Ctx &c, int cap, bool mixed, int maxnew) {
         }
     }
     if (mixed && (b->cap32 < maxnew || !b->v32)) {
+        drop_graphs(b);
         cudaFree(b->v32);
         cudaFree(b->s32);
         b->cap32 = maxnew;
@@ -390,21 +528,21 @@ static jci_status ensure_buffers(Ctx &c, int cap, bool mixed, int maxnew) {
 // C[i0 .. i0+m) = H V[i0 .. i0+m) in the requested precision
 static jci_status sigma_block(Ctx &c, int i0, int m, bool fp32) {
     DavidsonBuffers *b = c.b;
-    auto t0 = std::chrono::steady_clock::now();
     cudaEvent_t e0 = c.d->ev0, e1 = c.d->ev1;
     jci_status r;
+    double ms_call = 0.0;
     if (fp32) {
         for (int k0 = 0; k0 < m; k0 += b->cap32) {
             int mm = std::min(b->cap32, m - k0);
             k_d2f<<<grid_for(c.n), 256, 0, c.st>>>(b->V + (i0 + k0) * c.ld, b->v32, c.n, c.ld,
-                                                   c.ld, mm);
+                                                   c.ld, mm, nullptr);
             if ((r = device_sigma(c.s, mm, b->v32, b->s32, c.ld, JCI_FP32, c.st))) return r;
             float ms = 0.f;
             JCI_CUDA(cudaEventSynchronize(e1));
             JCI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            c.sigma_ms += ms;
+            ms_call += ms;
             k_f2d<<<grid_for(c.n), 256, 0, c.st>>>(b->s32, b->C + (i0 + k0) * c.ld, c.n, c.ld,
-                                                   c.ld, mm);
+                                                   c.ld, mm, nullptr);
         }
         c.fp32_vecs += m;
     } else {
@@ -414,9 +552,10 @@ static jci_status sigma_block(Ctx &c, int i0, int m, bool fp32) {
         float ms = 0.f;
         JCI_CUDA(cudaEventSynchronize(e1));
         JCI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        c.sigma_ms += ms;
+        ms_call = ms;
     }
-    (void)t0;
+    c.sigma_ms += ms_call;
+    c.ms_per_vec[fp32 ? 1 : 0] = ms_call / m;
     c.sigma_calls++;
     c.sigma_vecs += m;
     JCI_CUDA(cudaGetLastError());
@@ -424,13 +563,14 @@ static jci_status sigma_block(Ctx &c, int i0, int m, bool fp32) {
 }
 
 // out[i*p + j] = X_i . Y_j on the device (i < m <= 64, j < p <= 16)
-static jci_status gram(Ctx &c, const double *X, int m, const double *Y, int p, double *out) {
+static jci_status gram(Ctx &c, const double *X, int m, const double *Y, int p, double *out,
+                       GramDev gd = GramDev()) {
     if (m < 1 || m > kGramRows || p < 1 || p > kGramCols) return JCI_ERR_ARG;
     long long chunk = ((c.n + kDotBlocks - 1) / kDotBlocks + 63) / 64 * 64;
     int nb = (int)((c.n + chunk - 1) / chunk);
     gram_kernel((m + 7) / 8, (p + 7) / 8)<<<nb, 256, 0, c.st>>>(X, m, Y, p, c.ld, c.n, chunk,
-                                                                 c.b->partial);
-    k_gram_finish<<<m * p, 32, 0, c.st>>>(c.b->partial, nb, m * p, out);
+                                                                 c.b->partial, gd);
+    k_gram_finish<<<m * p, 32, 0, c.st>>>(c.b->partial, nb, m * p, out, gd, p);
     JCI_CUDA(cudaGetLastError());
     return JCI_OK;
 }
@@ -473,7 +613,7 @@ static jci_status rayleigh_ritz(Ctx &c, int m, const std::vector<double> &G,
     // the attribute is per device; setting it again is harmless and cheap
     JCI_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(2 * kMaxKry * (kMaxKry + 1) * sizeof(double))));
-    k_jacobi<<<1, 32, smem, c.st>>>(b->G, m, kMaxKry, b->eval, b->evec, c.d_info);
+    k_jacobi<<<1, 32, smem, c.st>>>(b->G, m, kMaxKry, b->eval, b->evec, c.d_info, nullptr);
     int info = 0;
     JCI_CUDA(cudaMemcpyAsync(w.data(), b->eval, m * sizeof(double), cudaMemcpyDeviceToHost, c.st));
     JCI_CUDA(cudaMemcpyAsync(Y.data(), b->evec, kMaxKry * kMaxKry * sizeof(double),
@@ -494,7 +634,7 @@ static jci_status lincomb(Ctx &c, double *out, const double *X, const double *a,
     JCI_CUDA(cudaMemcpyAsync(b->coef, cc.data(), 2 * kMaxKry * sizeof(double),
                              cudaMemcpyHostToDevice, c.st));
     k_lincomb<<<grid_for(c.n), 256, 0, c.st>>>(out, c.n, c.ld, X, b->coef, mx, Yv,
-                                               b->coef + kMaxKry, my);
+                                               b->coef + kMaxKry, my, nullptr);
     JCI_CUDA(cudaGetLastError());
     return JCI_OK;
 }
@@ -543,16 +683,16 @@ static jci_status orthonormalize(Ctx &c, double *t, int m, int npass, double *nr
     jci_status r;
     if (prescale) {
         if ((r = dots(c, t, 1, t, nullptr))) return r;
-        k_normalize<<<grid_for(c.n), 256, 0, c.st>>>(t, c.n, b->dots);
+        k_normalize<<<grid_for(c.n), 256, 0, c.st>>>(t, c.n, b->dots, nullptr);
     }
     for (int p = 0; p < npass && m > 0; p++) {
         if ((r = dots(c, b->V, m, t, nullptr))) return r;
-        k_orth_update<<<grid_for(c.n), 256, 0, c.st>>>(t, c.n, c.ld, b->V, b->dots, m);
+        k_orth_update<<<grid_for(c.n), 256, 0, c.st>>>(t, c.n, c.ld, b->V, b->dots, m, nullptr);
     }
     if ((r = dots(c, t, 1, t, nullptr))) return r;
     double h = 0.0;
     JCI_CUDA(cudaMemcpyAsync(&h, b->dots, sizeof(double), cudaMemcpyDeviceToHost, c.st));
-    k_normalize<<<grid_for(c.n), 256, 0, c.st>>>(t, c.n, b->dots);
+    k_normalize<<<grid_for(c.n), 256, 0, c.st>>>(t, c.n, b->dots, nullptr);
     JCI_CUDA(cudaStreamSynchronize(c.st));
     JCI_CUDA(cudaGetLastError());
     *nrm = sqrt(h);
@@ -597,11 +737,190 @@ static jci_status initial_vectors(Ctx &c, const jci_davidson_opts *o) {
     return JCI_OK;
 }
 
+// ---- iterations of the root-sequential schedule ---------------------------
+//
+// One iteration: residual of the current root, its norm test, the
+// preconditioned correction, one classical Gram-Schmidt pass, sigma of the
+// new basis vector, the new row of the subspace matrix and the Jacobi
+// eigensolve.  host_iteration launches these kernels with sizes known on
+// the host and reads the residual norm back; the captured iteration
+// (enqueue_iteration) runs the same kernels in the same order with every
+// size and decision kept in the device control block, so a batch of graph
+// launches needs one host synchronisation instead of five per iteration and
+// gives bitwise the same numbers.
+//
+// event: 0 vector added, 1 residual of root croot below tol (nothing added),
+// 2 basis full.
+
+static void print_iteration(const Ctx &c, int citer, int root, double theta, double rn,
+                            bool fp32) {
+    printf("  iter %4d  root %d  E = %18.12f  ||r|| = %.3e%s\n", citer, root,
+           theta + c.s->nucrep + c.s->frzcore, rn, fp32 ? "  (fp32 sigma)" : "");
+}
+
+static jci_status host_iteration(Ctx &c, const jci_davidson_opts *o, bool fp32, int croot,
+                                 double tol, int &ckdim, int &citer, double &rnorm,
+                                 std::vector<double> &G, std::vector<double> &w,
+                                 std::vector<double> &Y, int *event) {
+    DavidsonBuffers *b = c.b;
+    std::vector<double> yc(kMaxKry), ycv(kMaxKry);
+    jci_status r;
+    double th = w[croot - 1];
+    for (int i = 0; i < ckdim; i++) {
+        yc[i] = Y[(croot - 1) * kMaxKry + i];
+        ycv[i] = -th * yc[i];
+    }
+    if ((r = lincomb(c, b->r, b->C, yc.data(), ckdim, b->V, ycv.data(), ckdim))) return r;
+    double rn2 = 0.0;
+    if ((r = dots(c, b->r, 1, b->r, &rn2))) return r;
+    rnorm = sqrt(rn2);
+    if (o->printlvl > 0) print_iteration(c, citer, croot, th, rnorm, fp32);
+    if (rnorm < tol) {
+        *event = 1;
+        return JCI_OK;
+    }
+    k_precond<<<grid_for(c.n), 256, 0, c.st>>>(b->r, c.d->hd, th, b->t, c.n, nullptr);
+    double nn;
+    if ((r = orthonormalize(c, b->t, ckdim, 1, &nn))) return r;
+    JCI_CUDA(cudaMemcpyAsync(b->V + ckdim * c.ld, b->t, c.n * sizeof(double),
+                             cudaMemcpyDeviceToDevice, c.st));
+    if ((r = sigma_block(c, ckdim, 1, fp32))) return r;
+    ckdim++;
+    if ((r = gram_rows(c, ckdim - 1, ckdim, G))) return r;
+    if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
+    citer++;
+    *event = ckdim >= o->krymax ? 2 : 0;
+    return JCI_OK;
+}
+
+static jci_status enqueue_iteration(Ctx &c, bool fp32, int kmax) {
+    DavidsonBuffers *b = c.b;
+    DavCtl *ctl = b->ctl;
+    const int *stop = &ctl->stop;
+    const unsigned g = grid_for(c.n);
+    GramDev one, basis, with_new;
+    one.stop = basis.stop = with_new.stop = stop;
+    basis.mdev = with_new.mdev = &ctl->ckdim;
+    with_new.madd = 1;
+    jci_status r;
+    k_it_begin<<<1, 64, 0, c.st>>>(ctl, b->eval, b->evec, b->coef);
+    k_lincomb<<<g, 256, 0, c.st>>>(b->r, c.n, c.ld, b->C, b->coef, 0, b->V, b->coef + kMaxKry,
+                                   0, ctl);
+    if ((r = gram(c, b->r, 1, b->r, 1, b->dots, one))) return r;
+    k_it_check<<<1, 1, 0, c.st>>>(ctl, b->dots, b->hist);
+    k_precond<<<g, 256, 0, c.st>>>(b->r, c.d->hd, 0.0, b->t, c.n, ctl);
+    // the row counts below come from the control block; kmax bounds them
+    if ((r = gram(c, b->V, kmax, b->t, 1, b->dots, basis))) return r;
+    k_orth_update<<<g, 256, 0, c.st>>>(b->t, c.n, c.ld, b->V, b->dots, 0, ctl);
+    if ((r = gram(c, b->t, 1, b->t, 1, b->dots, one))) return r;
+    k_normalize<<<g, 256, 0, c.st>>>(b->t, c.n, b->dots, stop);
+    k_it_store<<<g, 256, 0, c.st>>>(b->V, c.ld, 0, b->t, c.n, ctl);
+    if (fp32) {
+        k_d2f<<<g, 256, 0, c.st>>>(b->t, b->v32, c.n, c.ld, c.ld, 1, stop);
+        if ((r = device_sigma(c.s, 1, b->v32, b->s32, c.ld, JCI_FP32, c.st))) return r;
+        k_f2d<<<g, 256, 0, c.st>>>(b->s32, b->cnew, c.n, c.ld, c.ld, 1, stop);
+    } else {
+        if ((r = device_sigma(c.s, 1, b->t, b->cnew, c.ld, JCI_FP64, c.st))) return r;
+    }
+    k_it_store<<<g, 256, 0, c.st>>>(b->C, c.ld, 0, b->cnew, c.n, ctl);
+    if ((r = gram(c, b->C, kmax, b->t, 1, b->dots, with_new))) return r;
+    k_it_append<<<1, 64, 0, c.st>>>(ctl, b->dots, b->G);
+    k_jacobi<<<1, 32, 2 * (size_t)kmax * (kmax + 1) * sizeof(double), c.st>>>(
+        b->G, 0, kMaxKry, b->eval, b->evec, b->info, ctl);
+    k_it_end<<<1, 1, 0, c.st>>>(ctl, b->info, kmax);
+    JCI_CUDA(cudaGetLastError());
+    return JCI_OK;
+}
+
+// Capture (once per precision, basis size and sigma plan) the iteration as
+// a CUDA graph.  The sigma kernels see the control block's stop flag.
+static jci_status ensure_graph(Ctx &c, bool fp32, int kmax) {
+    DavidsonBuffers *b = c.b;
+    const int p = fp32 ? 1 : 0;
+    int plan[4] = {0, 0, 0, 0};
+    if (c.d->fci) {
+        float ms = 0.f;
+        fci_tuning(c.s, fp32 ? JCI_FP32 : JCI_FP64, &plan[0], &plan[1], &plan[2], &plan[3], &ms);
+    }
+    if (b->gexec[p] && b->gkmax[p] == kmax && memcmp(plan, b->gplan[p], sizeof plan) == 0)
+        return JCI_OK;
+    if (b->gexec[p]) {
+        cudaGraphExecDestroy(b->gexec[p]);
+        b->gexec[p] = nullptr;
+    }
+    JCI_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(2 * kMaxKry * (kMaxKry + 1) * sizeof(double))));
+    cudaGraph_t graph = nullptr;
+    JCI_CUDA(cudaStreamBeginCapture(c.st, cudaStreamCaptureModeRelaxed));
+    c.d->sigma_skip = &b->ctl->stop;
+    jci_status r = enqueue_iteration(c, fp32, kmax);
+    c.d->sigma_skip = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c.st, &graph);
+    if (r == JCI_OK && e != cudaSuccess) r = cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+    if (r == JCI_OK) {
+        e = cudaGraphInstantiate(&b->gexec[p], graph, 0);
+        if (e != cudaSuccess) {
+            b->gexec[p] = nullptr;
+            r = cuda_fail(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+        }
+    }
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (r) return r;
+    b->gkmax[p] = kmax;
+    memcpy(b->gplan[p], plan, sizeof plan);
+    return JCI_OK;
+}
+
+// Launch the captured iteration kmax - ckdim times (the last launch fills
+// the basis at the latest), then read the control block, the history and
+// the subspace state back in one synchronisation.
+static jci_status graph_iterations(Ctx &c, const jci_davidson_opts *o, bool fp32, int croot,
+                                   double tol, int &ckdim, int &citer, double &rnorm,
+                                   std::vector<double> &G, std::vector<double> &w,
+                                   std::vector<double> &Y, int *event) {
+    DavidsonBuffers *b = c.b;
+    const int kmax = o->krymax, p = fp32 ? 1 : 0;
+    jci_status r = ensure_graph(c, fp32, kmax);
+    if (r) return r;
+    DavCtl h{};
+    h.ckdim = ckdim;
+    h.croot = croot - 1;
+    h.tol = tol;
+    JCI_CUDA(cudaMemcpyAsync(b->ctl, &h, sizeof h, cudaMemcpyHostToDevice, c.st));
+    for (int k = ckdim; k < kmax; k++) JCI_CUDA(cudaGraphLaunch(b->gexec[p], c.st));
+    std::vector<DavHist> hist(kHist);
+    JCI_CUDA(cudaMemcpyAsync(&h, b->ctl, sizeof h, cudaMemcpyDeviceToHost, c.st));
+    JCI_CUDA(cudaMemcpyAsync(hist.data(), b->hist, kHist * sizeof(DavHist),
+                             cudaMemcpyDeviceToHost, c.st));
+    JCI_CUDA(cudaMemcpyAsync(w.data(), b->eval, kMaxKry * sizeof(double), cudaMemcpyDeviceToHost,
+                             c.st));
+    JCI_CUDA(cudaMemcpyAsync(Y.data(), b->evec, kMaxKry * kMaxKry * sizeof(double),
+                             cudaMemcpyDeviceToHost, c.st));
+    JCI_CUDA(cudaMemcpyAsync(G.data(), b->G, kMaxKry * kMaxKry * sizeof(double),
+                             cudaMemcpyDeviceToHost, c.st));
+    JCI_CUDA(cudaStreamSynchronize(c.st));
+    const int nh = std::min(h.nhist, kHist);
+    for (int i = 0; i < nh; i++) {
+        rnorm = hist[i].rnorm;
+        if (o->printlvl > 0)
+            print_iteration(c, citer + i, hist[i].root + 1, hist[i].theta, hist[i].rnorm, fp32);
+    }
+    ckdim = h.ckdim;
+    citer += h.iters;
+    c.sigma_calls += h.iters;
+    c.sigma_vecs += h.iters;
+    if (fp32) c.fp32_vecs += h.iters;
+    c.sigma_ms += h.iters * c.ms_per_vec[p];
+    if (h.stop == 3) return JCI_ERR_LINALG;
+    *event = h.stop == 1 ? 1 : 2;
+    return JCI_OK;
+}
+
 static jci_status run_sequential(Ctx &c, const jci_davidson_opts *o, bool mixed,
                                  std::vector<double> &w, std::vector<double> &Y, int &ckdim,
                                  int &citer, int &converged, double &rnorm) {
-    DavidsonBuffers *b = c.b;
-    std::vector<double> G(kMaxKry * kMaxKry, 0.0), yc(kMaxKry), ycv(kMaxKry);
+    std::vector<double> G(kMaxKry * kMaxKry, 0.0);
     int kmin = o->krymin, kmax = o->krymax, nroots = o->nroots;
     bool fp32 = mixed;
     // The reference recomputes every sigma vector after a collapse
@@ -625,21 +944,22 @@ static jci_status run_sequential(Ctx &c, const jci_davidson_opts *o, bool mixed,
         }
         if ((r = gram_rows(c, 0, ckdim, G))) return r;
         if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
-        while (ckdim < kmax) {
-            double th = w[croot - 1];
-            for (int i = 0; i < ckdim; i++) {
-                yc[i] = Y[(croot - 1) * kMaxKry + i];
-                ycv[i] = -th * yc[i];
+        for (;;) {
+            int event = 2;
+            if (ckdim < kmax) {
+                r = o->host_loop
+                        ? host_iteration(c, o, fp32, croot, tol, ckdim, citer, rnorm, G, w, Y,
+                                         &event)
+                        : graph_iterations(c, o, fp32, croot, tol, ckdim, citer, rnorm, G, w,
+                                           Y, &event);
+                if (r) return r;
             }
-            if ((r = lincomb(c, b->r, b->C, yc.data(), ckdim, b->V, ycv.data(), ckdim)))
-                return r;
-            double rn2 = 0.0;
-            if ((r = dots(c, b->r, 1, b->r, &rn2))) return r;
-            rnorm = sqrt(rn2);
-            if (o->printlvl > 0)
-                printf("  iter %4d  root %d  E = %18.12f  ||r|| = %.3e%s\n", citer, croot,
-                       th + c.s->nucrep + c.s->frzcore, rnorm, fp32 ? "  (fp32 sigma)" : "");
-            cflag = rnorm < tol ? (croot < nroots ? 1 : 2) : 0;
+            if (event == 0) continue;
+            if (event == 2) {
+                cflag = 0;
+                break;
+            }
+            cflag = croot < nroots ? 1 : 2;
             if (cflag == 2 && fp32) {
                 fp32 = false;
                 tol = o->restol;
@@ -648,21 +968,8 @@ static jci_status run_sequential(Ctx &c, const jci_davidson_opts *o, bool mixed,
                 if ((r = switch_to_fp64(c, ckdim, kmin, G, w, Y))) return r;
                 continue;
             }
-            if (cflag == 2) break;
-            if (cflag == 1) {
-                croot++;
-                break;
-            }
-            k_precond<<<grid_for(c.n), 256, 0, c.st>>>(b->r, c.d->hd, th, b->t, c.n);
-            double nn;
-            if ((r = orthonormalize(c, b->t, ckdim, 1, &nn))) return r;
-            JCI_CUDA(cudaMemcpyAsync(b->V + ckdim * c.ld, b->t, c.n * sizeof(double),
-                                     cudaMemcpyDeviceToDevice, c.st));
-            if ((r = sigma_block(c, ckdim, 1, fp32))) return r;
-            ckdim++;
-            if ((r = gram_rows(c, ckdim - 1, ckdim, G))) return r;
-            if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
-            citer++;
+            if (cflag == 1) croot++;
+            break;
         }
         if ((r = collapse(c, ckdim, kmin, Y, !recompute))) return r;
         ckdim = kmin;
@@ -737,7 +1044,7 @@ static jci_status run_block(Ctx &c, const jci_davidson_opts *o, bool mixed,
                 ycv[i] = -th * yc[i];
             }
             if ((r = lincomb(c, b->r, b->C, yc.data(), ckdim, b->V, ycv.data(), ckdim))) return r;
-            k_precond<<<grid_for(c.n), 256, 0, c.st>>>(b->r, c.d->hd, th, b->t, c.n);
+            k_precond<<<grid_for(c.n), 256, 0, c.st>>>(b->r, c.d->hd, th, b->t, c.n, nullptr);
             double nn;
             if ((r = orthonormalize(c, b->t, ckdim + added, 2, &nn, true))) return r;
             if (!(nn > 1e-8)) continue;  // correction (numerically) inside the space
@@ -774,7 +1081,7 @@ jci_status davidson(jci_space *s, const jci_davidson_opts *o, double *energies, 
     int maxnew = std::max(o->krymin, o->nroots);
     jci_status r = ensure_buffers(c, o->krymax, mixed, maxnew);
     if (r) return r;
-    JCI_CUDA(cudaMalloc(&c.d_info, sizeof(int)));
+    c.d_info = c.b->info;
     std::vector<double> w(kMaxKry, 0.0), Y(kMaxKry * kMaxKry, 0.0);
     int ckdim = 0, citer = 0, conv = 0;
     double rnorm = 0.0;
@@ -785,7 +1092,6 @@ jci_status davidson(jci_space *s, const jci_davidson_opts *o, double *energies, 
         else
             r = run_sequential(c, o, mixed, w, Y, ckdim, citer, conv, rnorm);
     }
-    cudaFree(c.d_info);
     if (r) return r;
     double core = s->nucrep + s->frzcore;
     for (int k = 0; k < o->nroots; k++) energies[k] = w[k] + core;

@@ -46,6 +46,7 @@ SpaceView make_view(const DeviceState *d) {
     v.pairidx = d->pairidx;
     v.pqg = d->pqg;
     v.ndets = 0;
+    v.skip = d->sigma_skip;
     const SpinTables *t[2] = {&d->t[0], &d->t[1]};
     SpaceView::Spin *o[2] = {&v.a, &v.b};
     for (int s = 0; s < 2; s++) {
@@ -327,7 +328,7 @@ __global__ void __launch_bounds__(128) k_sigma_generic(SpaceView v, const T *__r
                                                        const T *__restrict__ V, T *__restrict__ S,
                                                        long long ld, int nvec) {
     long long d = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= v.ndets) return;
+    if (d >= v.ndets || (v.skip && *v.skip)) return;
     int k = 0;
     while (k + 1 < v.npq && v.pqoff[k + 1] <= d) k++;
     int pg = v.pqg[2 * k], qg = v.pqg[2 * k + 1];
@@ -425,7 +426,11 @@ jci_status device_sigma(jci_space *s, int nvec, const void *vin, void *sout, lon
     if (!s->have_ints) return JCI_ERR_STATE;
     if (nvec < 1 || ld < s->ndets || !vin || !sout) return JCI_ERR_ARG;
     cudaStream_t st = stream ? (cudaStream_t)stream : d->stream;
-    JCI_CUDA(cudaEventRecord(d->ev0, st));
+    // no timing events while the stream is being captured into a graph
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    JCI_CUDA(cudaStreamIsCapturing(st, &cap));
+    const bool timed = cap == cudaStreamCaptureStatusNone;
+    if (timed) JCI_CUDA(cudaEventRecord(d->ev0, st));
     jci_status r = JCI_OK;
     if (d->single_group && fci_supported(s)) {
         r = fci_sigma(s, nvec, vin, sout, ld, precision, st);
@@ -438,7 +443,7 @@ jci_status device_sigma(jci_space *s, int nvec, const void *vin, void *sout, lon
     }
     if (r != JCI_OK) return r;
     JCI_CUDA(cudaGetLastError());
-    JCI_CUDA(cudaEventRecord(d->ev1, st));
+    if (timed) JCI_CUDA(cudaEventRecord(d->ev1, st));
     return JCI_OK;
 }
 

@@ -77,11 +77,17 @@ struct DeviceState {
     size_t io_bytes = 0;
     struct FciTables *fci = nullptr;   // single-group fast path (jci_fci.cu)
     struct DavidsonBuffers *dav = nullptr;  // jci_davidson.cu
+    // Device flag read by every sigma kernel at entry: when nonzero the
+    // kernel returns at once.  Set while a Davidson iteration is captured
+    // into a CUDA graph, so that iterations launched after the solve has
+    // stopped cost no sigma work; null otherwise.
+    const int *sigma_skip = nullptr;
 };
 
 // Kernel-facing view of a space (POD, passed by value).
 struct SpaceView {
     long long ndets;
+    const int *skip;  // DeviceState::sigma_skip
     int npq, qegrps, norb, npair;
     const long long *pqoff;
     const int *pairidx;

@@ -121,6 +121,7 @@ struct FciArgs {
     const T *dHA, *dHB;
     const T *hd;                  // <i|H|i>
     const T *m2;                  // packed (pq|rs)
+    const int *skip;              // DeviceState::sigma_skip
 };
 
 template <typename T>
@@ -131,6 +132,7 @@ __device__ __forceinline__ T flip(T w, uint32_t neg) {
 template <typename T, int ITEMS>
 __global__ void __launch_bounds__(ITEMS <= 2 ? 1024 : 512)
     k_sigma_fci(FciArgs<T> a, const T *__restrict__ V, T *__restrict__ S) {
+    if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *rows = reinterpret_cast<T *>(smem_raw);         // (1 + R) x nb
     T *vrow = rows + (size_t)(1 + a.R) * a.nb;         // R x npair
@@ -145,26 +147,35 @@ __global__ void __launch_bounds__(ITEMS <= 2 ? 1024 : 512)
     for (int p = tid; p < a.npair; p += nt) jrow[p] = a.jA[(long long)p * a.na + Ia];
     __syncthreads();
 
+    // excitation index outer, the thread's ITEMS columns inner (unrolled):
+    // ITEMS independent table loads in flight per excitation
     T acc[ITEMS];
 #pragma unroll
     for (int it = 0; it < ITEMS; it++) {
         int Ib = tid + it * nt;
-        acc[it] = T(0);
-        if (Ib >= nb) continue;
-        T x = a.hd[(long long)Ia * nb + Ib] * rows[Ib];
-        // beta singles within the row (hmatels_1x with alpha as the other string)
-        for (int f = 0; f < a.sb; f++) {
+        acc[it] = Ib < nb ? a.hd[(long long)Ia * nb + Ib] * rows[Ib] : T(0);
+    }
+    // beta singles within the row (hmatels_1x with alpha as the other string)
+    for (int f = 0; f < a.sb; f++) {
+#pragma unroll
+        for (int it = 0; it < ITEMS; it++) {
+            int Ib = tid + it * nt;
+            if (Ib >= nb) continue;
             long long o = (long long)f * nb + Ib;
             uint32_t e = a.fsB[o];
             T h = a.a1B[o] + jrow[a.fpB[o]];
-            x += flip(h, e >> 31) * rows[e & 0x3fffffffu];
+            acc[it] += flip(h, e >> 31) * rows[e & 0x3fffffffu];
         }
-        // beta doubles within the row
-        for (int f = 0; f < a.db; f++) {
+    }
+    // beta doubles within the row
+    for (int f = 0; f < a.db; f++) {
+#pragma unroll
+        for (int it = 0; it < ITEMS; it++) {
+            int Ib = tid + it * nt;
+            if (Ib >= nb) continue;
             long long o = (long long)f * nb + Ib;
-            x += a.dHB[o] * rows[a.dJB[o]];
+            acc[it] += a.dHB[o] * rows[a.dJB[o]];
         }
-        acc[it] = x;
     }
 
     // alpha singles (with alpha x beta doubles), R staged rows at a time
@@ -201,22 +212,29 @@ __global__ void __launch_bounds__(ITEMS <= 2 ? 1024 : 512)
                 T h = coef[r] + flip(a.jB[(long long)pas[r] * nb + Ib], sgn[r]);
                 x += h * rows[(size_t)(1 + r) * nb + Ib];
             }
-            for (int f = 0; f < a.sb; f++) {
+            acc[it] = x;
+        }
+        for (int f = 0; f < a.sb; f++) {
+#pragma unroll
+            for (int it = 0; it < ITEMS; it++) {
+                int Ib = tid + it * nt;
+                if (Ib >= nb) continue;
                 long long o = (long long)f * nb + Ib;
                 uint32_t e = a.fsB[o];
                 int J = (int)(e & 0x3fffffffu), pr = a.fpB[o];
                 uint32_t neg = e >> 31;
                 const T *rr = rows + nb + J;
                 const T *vv = vrow + pr;
+                T x = T(0);
 #pragma unroll 4
-                for (int r = 0; r < nr; r++)
-                    x += flip(vv[(size_t)r * a.npair], neg) * rr[(size_t)r * nb];
+                for (int r = 0; r < nr; r++) x += vv[(size_t)r * a.npair] * rr[(size_t)r * nb];
+                acc[it] += flip(x, neg);
             }
-            acc[it] = x;
         }
     }
 
     // alpha doubles: rows streamed from global memory
+#pragma unroll 2
     for (int f = 0; f < a.da; f++) {
         long long o = (long long)f * a.na + Ia;
         int Ja = a.dJA[o];
@@ -263,11 +281,13 @@ struct MixArgs {
     const T *a1A;
     const T *m2;
     const uint64_t *occB;
+    const int *skip;
 };
 
 template <typename T, int TM>
 __global__ void __launch_bounds__(kMixThreads)
     k_sigma_mixed(MixArgs<T> a, const T *__restrict__ V, T *__restrict__ S, T *__restrict__ Tbuf) {
+    if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int MP = 16 * TM;
     const int K = a.sa;
@@ -386,11 +406,13 @@ struct Mix2Args {
     const T *a1A;
     const T *m2;
     const uint64_t *occB;
+    const int *skip;
 };
 
 template <typename T, int TM>
 __global__ void __launch_bounds__(kMixThreads)
     k_sigma_mixed2(Mix2Args<T> a, const T *__restrict__ V, T *__restrict__ S) {
+    if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int MP = 16 * TM;
     const int K = a.sa, nb = a.nb;
@@ -514,13 +536,23 @@ static size_t mix2_smem(int K, int TM, int mrows, int nb, size_t w) {
 // memory, so one load of a beta excitation entry serves RB rows) and the
 // alpha doubles (rows streamed from global memory).  The alpha singles are
 // added by k_sigma_mixed afterwards.
+//
+// Loop order: the excitation index is the outer loop and the ITEMS columns
+// of a thread the inner, unrolled one, so each warp has ITEMS independent
+// table loads (and shared-memory gathers) in flight per excitation instead
+// of one.  The alpha-double list of every row (target, value) is staged in
+// shared memory first, so streaming a row c(Ja, :) waits on one global
+// load, not two.
 
 template <typename T, int ITEMS, int RB>
 __global__ void __launch_bounds__(ITEMS * RB <= 4 ? 1024 : 512)
     k_sigma_rows(FciArgs<T> a, const T *__restrict__ V, T *__restrict__ S) {
+    if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *rows = reinterpret_cast<T *>(smem_raw);   // RB x nb
     T *jrow = rows + (size_t)RB * a.nb;          // RB x npair
+    T *dh = jrow + (size_t)RB * a.npair;         // RB x da  alpha-double values
+    int *dj = reinterpret_cast<int *>(dh + (size_t)RB * a.da);  // RB x da targets
     const int nb = a.nb, tid = threadIdx.x, nt = blockDim.x;
     const int Ia0 = blockIdx.x * RB;
     const int nr = min(RB, a.na - Ia0);
@@ -529,6 +561,11 @@ __global__ void __launch_bounds__(ITEMS * RB <= 4 ? 1024 : 512)
         for (int i = tid; i < nb; i += nt) rows[(size_t)r * nb + i] = crow[i];
         for (int p = tid; p < a.npair; p += nt)
             jrow[(size_t)r * a.npair + p] = a.jA[(long long)p * a.na + Ia0 + r];
+        for (int f = tid; f < a.da; f += nt) {
+            long long o = (long long)f * a.na + Ia0 + r;
+            dh[(size_t)r * a.da + f] = a.dHA[o];
+            dj[(size_t)r * a.da + f] = a.dJA[o];
+        }
     }
     __syncthreads();
     T acc[ITEMS][RB];
@@ -536,12 +573,18 @@ __global__ void __launch_bounds__(ITEMS * RB <= 4 ? 1024 : 512)
     for (int it = 0; it < ITEMS; it++) {
         int Ib = tid + it * nt;
 #pragma unroll
-        for (int r = 0; r < RB; r++) acc[it][r] = T(0);
-        if (Ib >= nb) continue;
-#pragma unroll
         for (int r = 0; r < RB; r++)
-            if (r < nr) acc[it][r] = a.hd[(long long)(Ia0 + r) * nb + Ib] * rows[(size_t)r * nb + Ib];
-        for (int f = 0; f < a.sb; f++) {
+            acc[it][r] = Ib < nb && r < nr
+                             ? a.hd[(long long)(Ia0 + r) * nb + Ib] * rows[(size_t)r * nb + Ib]
+                             : T(0);
+    }
+    // beta singles within the rows (hmatels_1x with the alpha string's
+    // Coulomb row jrow)
+    for (int f = 0; f < a.sb; f++) {
+#pragma unroll
+        for (int it = 0; it < ITEMS; it++) {
+            int Ib = tid + it * nt;
+            if (Ib >= nb) continue;
             long long o = (long long)f * nb + Ib;
             uint32_t e = a.fsB[o];
             T h = a.a1B[o];
@@ -552,7 +595,13 @@ __global__ void __launch_bounds__(ITEMS * RB <= 4 ? 1024 : 512)
                 acc[it][r] += flip(h + jrow[(size_t)r * a.npair + pr], neg) *
                               rows[(size_t)r * nb + J];
         }
-        for (int f = 0; f < a.db; f++) {
+    }
+    // beta doubles within the rows
+    for (int f = 0; f < a.db; f++) {
+#pragma unroll
+        for (int it = 0; it < ITEMS; it++) {
+            int Ib = tid + it * nt;
+            if (Ib >= nb) continue;
             long long o = (long long)f * nb + Ib;
             T h = a.dHB[o];
             int J = a.dJB[o];
@@ -564,11 +613,10 @@ __global__ void __launch_bounds__(ITEMS * RB <= 4 ? 1024 : 512)
 #pragma unroll
     for (int r = 0; r < RB; r++) {
         if (r >= nr) break;
+#pragma unroll 2
         for (int f = 0; f < a.da; f++) {
-            long long o = (long long)f * a.na + Ia0 + r;
-            int Ja = a.dJA[o];
-            T h = a.dHA[o];
-            const T *src = V + (long long)Ja * nb;
+            const T h = dh[(size_t)r * a.da + f];
+            const T *src = V + (long long)dj[(size_t)r * a.da + f] * nb;
 #pragma unroll
             for (int it = 0; it < ITEMS; it++) {
                 int Ib = tid + it * nt;
@@ -588,8 +636,8 @@ __global__ void __launch_bounds__(ITEMS * RB <= 4 ? 1024 : 512)
     }
 }
 
-static size_t rows_smem(int nb, int npair, int RB, size_t w) {
-    return (size_t)RB * nb * w + (size_t)RB * npair * w + 16;
+static size_t rows_smem(int nb, int npair, int da, int RB, size_t w) {
+    return (size_t)RB * nb * w + (size_t)RB * npair * w + (size_t)RB * da * (w + 4) + 16;
 }
 
 static size_t mix_smem(int K, int TM, size_t w) {
@@ -693,7 +741,7 @@ static jci_status launch_one(const FciArgs<T> &a, int nt, size_t smem, int na, c
 template <typename T, int IT, int RB>
 static jci_status launch_rows_t(const FciArgs<T> &a, int nt, const T *v, T *o,
                                 cudaStream_t st) {
-    size_t smem = rows_smem(a.nb, a.npair, RB, sizeof(T));
+    size_t smem = rows_smem(a.nb, a.npair, a.da, RB, sizeof(T));
     JCI_CUDA(smem_optin(k_sigma_rows<T, IT, RB>));
     k_sigma_rows<T, IT, RB><<<(a.na + RB - 1) / RB, nt, smem, st>>>(a, v, o);
     return JCI_OK;
@@ -766,6 +814,7 @@ static jci_status launch_mixed(jci_space *s, const FciArgs<T> &fa, const T *v, T
     m.sa = fa.sa; m.sb = fa.sb; m.npair = fa.npair; m.mrows = fa.npair + 1;
     m.fsA = fa.fsA; m.fsB = fa.fsB; m.fpA = fa.fpA; m.fpB = fa.fpB;
     m.a1A = fa.a1A; m.m2 = fa.m2; m.occB = d->t[1].occ;
+    m.skip = fa.skip;
     int TM = (m.mrows + 15) / 16;
     MixKernel<T> kern = mixed_kernel<T>(TM);
     if (!kern) return JCI_ERR_SPACE;
@@ -825,6 +874,7 @@ static jci_status launch_mixed2(jci_space *s, const FciArgs<T> &fa, const T *v, 
     m.sa = fa.sa; m.sb = fa.sb; m.npair = fa.npair; m.mrows = fa.npair + 1;
     m.fsA = fa.fsA; m.fpA = fa.fpA; m.sortB = f->sortB;
     m.a1A = fa.a1A; m.m2 = fa.m2; m.occB = d->t[1].occ;
+    m.skip = fa.skip;
     int TM = (m.mrows + 15) / 16;
     Mix2Kernel<T> kern = mixed2_kernel<T>(TM);
     if (!kern || !f->sortB) return JCI_ERR_SPACE;
@@ -921,7 +971,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
         for (int nt : nts) {
             if (!useful(nt)) continue;
             for (int B : {1, 2, 4}) {
-                if (!rows_ok(f->nb, nt, B) || rows_smem(f->nb, f->npair, B, w) > f->smem_max)
+                if (!rows_ok(f->nb, nt, B) || rows_smem(f->nb, f->npair, f->da, B, w) > f->smem_max)
                     continue;
                 float ms = timeit([&] { return launch_rows<T>(ar, nt, B, v, o, st); });
                 if (ms < brow) { brow = ms; b1nt = nt; b1B = B; }
@@ -977,6 +1027,7 @@ static jci_status launch_fci(jci_space *s, int nvec, const T *V, T *S, long long
     a.npair = f->npair;
     a.R = 1;
     a.do_as = 1;
+    a.skip = d->sigma_skip;
     a.fsA = d->t[0].fsing; a.fsB = d->t[1].fsing;
     a.fpA = d->t[0].fspair; a.fpB = d->t[1].fspair;
     a.dJA = f->dblJ[0]; a.dJB = f->dblJ[1];
@@ -1022,7 +1073,7 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, 
     if (mode == 1 || mode == 2) {
         bool ok = mode == 1 ? mixed_possible(f, w) : mixed2_possible(f, w);
         if (!ok || !rows_ok(f->nb, nt, B) || R < 0 ||
-            rows_smem(f->nb, f->npair, B, w) > f->smem_max)
+            rows_smem(f->nb, f->npair, f->da, B, w) > f->smem_max)
             return JCI_ERR_ARG;
     } else {
         int items = (f->nb + nt - 1) / nt;
@@ -1084,6 +1135,7 @@ static jci_status sigma_noalloc(jci_space *s, const T *v, T *o, cudaStream_t st)
     a.npair = f->npair;
     a.R = 0;
     a.do_as = 0;
+    a.skip = nullptr;
     a.fsA = d->t[0].fsing; a.fsB = d->t[1].fsing;
     a.fpA = d->t[0].fspair; a.fpB = d->t[1].fspair;
     a.dJA = f->dblJ[0]; a.dJB = f->dblJ[1];
@@ -1103,6 +1155,7 @@ static jci_status sigma_noalloc(jci_space *s, const T *v, T *o, cudaStream_t st)
     m.sa = a.sa; m.sb = a.sb; m.npair = a.npair; m.mrows = a.npair + 1;
     m.fsA = a.fsA; m.fsB = a.fsB; m.fpA = a.fpA; m.fpB = a.fpB;
     m.a1A = a.a1A; m.m2 = a.m2; m.occB = d->t[1].occ;
+    m.skip = nullptr;
     size_t panel = (size_t)m.mrows * m.nbp * w;
     if (panel > kNoAllocScratchBytes) return JCI_ERR_SPACE;  // one row's panel must fit
     int TM = (m.mrows + 15) / 16;

@@ -95,6 +95,43 @@ def test_fci12_three_roots_all_schedules_agree():
     assert np.linalg.norm(res, axis=1).max() < 2e-8
 
 
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("prec", [jb.FP64, jb.MIXED])
+def test_graph_iterations_match_host_loop(name, prec):
+    """The CUDA-graph iterations (control state on the device, batches of
+    launches) and the host-driven iterations run the same kernels in the same
+    order: energies, vectors and iteration counts are bitwise equal."""
+    g = load(name)
+    s = space_for(g)
+    kmin, kmax, nroots, refdim = (int(x) for x in g["dav_opts"])
+    kw = dict(maxiter=500, krymin=kmin, krymax=kmax, nroots=nroots, refdim=refdim,
+              restol=1e-9, precision=prec)
+    rg = s.davidson(**kw)
+    rh = s.davidson(host_loop=True, **kw)
+    assert rg.converged and rh.converged
+    assert rg.stats.iterations == rh.stats.iterations
+    assert rg.stats.sigma_vectors == rh.stats.sigma_vectors
+    np.testing.assert_array_equal(rg.energies, rh.energies)
+    np.testing.assert_array_equal(rg.civec, rh.civec)
+    check(rg, g, tol=1e-10 if prec == jb.FP64 else 1e-8, ovl=1e-9 if prec == jb.FP64 else 1e-8)
+
+
+def test_graph_iterations_fci12():
+    """853 776 determinants, 3 roots: graph and host-driven reference
+    schedules agree bitwise."""
+    ints = workload_integrals("fci12_12")
+    m1, m2 = ints.packed()
+    s = jb.Space(12, 12)
+    s.set_integrals(m1, m2, ints.e_nuc, 0.0)
+    kw = dict(maxiter=500, krymin=6, krymax=24, nroots=3, refdim=12, restol=1e-8)
+    rg = s.davidson(**kw)
+    rh = s.davidson(host_loop=True, **kw)
+    assert rg.converged and rh.converged
+    assert rg.stats.iterations == rh.stats.iterations
+    np.testing.assert_array_equal(rg.energies, rh.energies)
+    np.testing.assert_array_equal(rg.civec, rh.civec)
+
+
 def test_restart_from_files(tmp_path, monkeypatch):
     """civec / ci.restart written like the reference; prediagr=3 restarts."""
     g = load("cas6_6")
