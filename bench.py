@@ -400,7 +400,7 @@ def run_serve(a):
         pos[sc] += 1
     N = len(seq)
     prec = jb.MIXED if a.serve_mixed else jb.FP64
-    kw = dict(krymin=4, krymax=16, refdim=8, restol=1e-8, maxiter=2000, precision=prec)
+    kw = dict(krymin=4, krymax=16, refdim=8, restol=1e-8, maxiter=5000, precision=prec)
 
     def submit(srv, r, warm):
         return srv.submit((r["m"], r["m"], 0, 0, r["m"], 0, 0), r["m1"], r["m2"], r["e_nuc"],
@@ -435,7 +435,7 @@ def run_serve(a):
         sp = spaces[m]
         ts = time.perf_counter()
         sp.set_integrals(r["m1"], r["m2"], r["e_nuc"], 0.0)
-        res = sp.davidson(maxiter=2000, krymin=4, krymax=16, nroots=r["nroots"], refdim=8,
+        res = sp.davidson(maxiter=5000, krymin=4, krymax=16, nroots=r["nroots"], refdim=8,
                           restol=1e-8, want_vectors=False)
         rows.append((m, time.perf_counter() - ts, res.stats.iterations,
                      res.stats.sigma_seconds))
@@ -473,11 +473,14 @@ def run_serve(a):
         ok = all(x.status == 0 and x.converged for x in res)
         rows = [(r["m"], x.solve_seconds, x.iterations, x.sigma_seconds)
                 for r, x in zip(seq, res)]
+        failed = [dict(scan=r["scan"], step=r["step"], cas=r["m"], nroots=r["nroots"],
+                       iterations=x.iterations, status=x.status, warm=x.warm_started)
+                  for r, x in zip(seq, res) if not (x.status == 0 and x.converged)]
         return dict(solves_per_s=N / (t1 - t0), wall_s=t1 - t0,
                     p50_ms=float(np.percentile(lat, 50) * 1e3),
                     p99_ms=float(np.percentile(lat, 99) * 1e3),
                     warm_started=int(sum(x.warm_started for x in res)), all_converged=ok,
-                    by_size=by_size(rows))
+                    not_converged=failed[:8], by_size=by_size(rows))
 
     one = play(1, 0.0)
     rate = 1.5 * one["solves_per_s"]

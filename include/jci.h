@@ -368,6 +368,52 @@ jci_status jci_write_vectors(const char *path, int dim, int len,
                              const double *v);
 jci_status jci_read_vectors(const char *path, int dim, int len, double *v);
 
+/* ---------------------------------------------------------------------
+ * Dyson orbitals between an (N+1)-electron and an N-electron CI
+ * wavefunction on the same orbitals (the pdycicalc program:
+ * run_pdycicalc.c:26, dysoncomp.c:103,220).
+ * --------------------------------------------------------------------- */
+
+/* &wavefcn0 / &wavefcn1 namelists of dycicalc.in (readnamelist.f90:47-50,
+ * defaults 0 as at :110-158). */
+typedef struct {
+        int electrons, orbitals, nfrozen, ndocc, nactive, nfrzvirt, xlevel;
+        int nstates;
+} jci_wavefcn;
+
+/* Read dycicalc.in (readwf0input / readwf1input / readdysoninput,
+ * ioutil.c:154-260): &wavefcn0 (N+1 electrons), &wavefcn1 (N electrons)
+ * and &dysonorbital states0 / states1 (five 1-based states each, default
+ * states0 = states1 = 1).  *nst0 / *nst1 receive the position of the last
+ * nonzero entry, as the reference counts them; states arrays hold 5. */
+jci_status jci_read_dycicalc(const char *path, jci_wavefcn *wf0,
+                             jci_wavefcn *wf1, int *states0, int *nst0,
+                             int *states1, int *nst1);
+
+/* Dyson orbitals (compute_dyson_orbital_a / _b and the sqrt(N+1)
+ * prefactor, run_pdycicalc.c:376-414).  s0 is the (N+1)-electron space,
+ * s1 the N-electron space (electrons one fewer, same orbitals, frozen,
+ * DOCC, active and frozen-virtual counts: check_wavefunction_input,
+ * run_pdycicalc.c:458).  v0 holds nstates0 x ndets(s0) and v1 nstates1 x
+ * ndets(s1) host vectors, state-major.  For every determinant of s0 and
+ * every electron of the spin whose count differs (beta when the N+1
+ * electron count is even, else alpha), the electron is removed; when the
+ * string and determinant exist in s1 the product
+ * v0[states0[j]] v1[states1[k]] is added to that orbital of Dyson orbital
+ * j*nst1 + k (no phase factor, as the reference).  dyorb receives
+ * (nst0*nst1) x orbitals values (orbitals of &wavefcn0, indexed by CI
+ * orbital number - 1).  Runs on the device; deterministic summation. */
+jci_status jci_dyson(jci_space *s0, jci_space *s1, const double *v0,
+                     int nstates0, const double *v1, int nstates1,
+                     const int *states0, int nst0, const int *states1,
+                     int nst1, double *dyorb);
+
+/* Write dysonorb.dat in the format of print_dysonorbitals_to_file
+ * (run_pdycicalc.c:674-712). */
+jci_status jci_write_dysonorb(const char *path, int ndyorbs, int orbs,
+                              const double *dyorb, const int *states0,
+                              int nst0, const int *states1, int nst1);
+
 #ifdef __cplusplus
 }
 #endif

@@ -116,6 +116,10 @@ def lib():
         L.jci_write_moints.argtypes = [ctypes.c_char_p, ip, vp, vp, dp, dp]
         L.jci_write_vectors.argtypes = [ctypes.c_char_p, ip, ip, vp]
         L.jci_read_vectors.argtypes = [ctypes.c_char_p, ip, ip, vp]
+        L.jci_read_dycicalc.argtypes = [ctypes.c_char_p, vp, vp, vp, ctypes.POINTER(ip), vp,
+                                        ctypes.POINTER(ip)]
+        L.jci_dyson.argtypes = [vp, vp, vp, ip, vp, ip, vp, ip, vp, ip, vp]
+        L.jci_write_dysonorb.argtypes = [ctypes.c_char_p, ip, ip, vp, vp, ip, vp, ip]
         _lib = L
     return _lib
 
@@ -158,6 +162,7 @@ class Space:
         (self.na, self.nb, self.norb, self.nastr, self.nbstr, self.pegrps,
          self.qegrps, self.npq, self.ndets, self.intorb) = (int(x) for x in sz)
         self.ndocc, self.nactv, self.xlvl = ndocc, nactive, xlevel
+        self.electrons, self.orbitals = electrons, orbitals
 
     def close(self):
         if getattr(self, "h", None):
@@ -404,3 +409,46 @@ def read_vectors(path, dim, length):
     v = np.zeros((dim, length))
     _check(lib().jci_read_vectors(str(path).encode(), dim, length, _p(v)), "read_vectors")
     return v
+
+
+class Wavefcn(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int) for k in ("electrons", "orbitals", "nfrozen", "ndocc",
+                                           "nactive", "nfrzvirt", "xlevel", "nstates")]
+
+    def general(self):
+        return (self.electrons, self.orbitals, self.nfrozen, self.ndocc, self.nactive,
+                self.nfrzvirt, self.xlevel)
+
+
+def read_dycicalc(path):
+    """dycicalc.in: (wavefcn0, wavefcn1, states0, states1), states 1-based
+    and truncated after the last nonzero entry as the reference counts."""
+    w0, w1 = Wavefcn(), Wavefcn()
+    s0, s1 = np.zeros(5, np.int32), np.zeros(5, np.int32)
+    n0, n1 = ctypes.c_int(0), ctypes.c_int(0)
+    _check(lib().jci_read_dycicalc(str(path).encode(), ctypes.byref(w0), ctypes.byref(w1),
+                                   _p(s0), ctypes.byref(n0), _p(s1), ctypes.byref(n1)),
+           "read_dycicalc")
+    return w0, w1, s0[:n0.value].copy(), s1[:n1.value].copy()
+
+
+def dyson(space0, space1, v0, v1, states0=(1,), states1=(1,)):
+    """Dyson orbitals between the (N+1)-electron space0 and the N-electron
+    space1 (jci_dyson): (len(states0) * len(states1)) x orbitals."""
+    v0 = np.ascontiguousarray(np.atleast_2d(v0), np.float64)
+    v1 = np.ascontiguousarray(np.atleast_2d(v1), np.float64)
+    st0 = np.ascontiguousarray(states0, np.int32)
+    st1 = np.ascontiguousarray(states1, np.int32)
+    out = np.zeros((len(st0) * len(st1), space0.orbitals))
+    _check(lib().jci_dyson(space0.h, space1.h, _p(v0), v0.shape[0], _p(v1), v1.shape[0],
+                           _p(st0), len(st0), _p(st1), len(st1), _p(out)), "dyson")
+    return out
+
+
+def write_dysonorb(path, dyorb, states0, states1):
+    dyorb = np.ascontiguousarray(np.atleast_2d(dyorb), np.float64)
+    st0 = np.ascontiguousarray(states0, np.int32)
+    st1 = np.ascontiguousarray(states1, np.int32)
+    _check(lib().jci_write_dysonorb(str(path).encode(), dyorb.shape[0], dyorb.shape[1],
+                                    _p(dyorb), _p(st0), len(st0), _p(st1), len(st1)),
+           "write_dysonorb")

@@ -1,4 +1,4 @@
-"""Build libjci.so (and the jci driver program) in-tree for sm_100a.
+"""Build libjci.so (and the jci / jci_dyson driver programs) in-tree for sm_100a.
 
     python -m jayci_b200.build [--force]
 
@@ -26,7 +26,9 @@ EXE = os.path.join(HERE, "jci")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["jci_space.cpp", "jci_io.cpp", "jci_api.cpp", "jci_server.cpp", "jci_device.cu", "jci_fci.cu",
-           "jci_davidson.cu"]
+           "jci_davidson.cu", "jci_dyson.cu"]
+# driver programs: (source, executable)
+PROGRAMS = [("jci_main.c", "jci"), ("jci_dyson_main.c", "jci_dyson")]
 
 
 def nvcc() -> str:
@@ -78,14 +80,15 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
-    main = os.path.join(CSRC, "jci_main.c")
-    if os.path.exists(main) and (force or _stale(EXE, [main, LIB, os.path.join(INCLUDE, "jci.h")])):
-        cmd = ["/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc", "-O2", "-std=gnu11",
-               "-I", INCLUDE, main, "-o", EXE, "-L", HERE, "-ljci",
-               "-Wl,-rpath,$ORIGIN", "-lm"]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"driver build failed: {' '.join(cmd)}\n{r.stderr}")
+    for src, exe in PROGRAMS:
+        main, out = os.path.join(CSRC, src), os.path.join(HERE, exe)
+        if force or _stale(out, [main, LIB, os.path.join(INCLUDE, "jci.h")]):
+            cmd = ["/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc", "-O2",
+                   "-std=gnu11", "-I", INCLUDE, main, "-o", out, "-L", HERE, "-ljci",
+                   "-Wl,-rpath,$ORIGIN", "-lm"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"driver build failed: {' '.join(cmd)}\n{r.stderr}")
     if verbose:
         print(LIB)
     return LIB

@@ -192,6 +192,26 @@ __global__ void __launch_bounds__(256)
         partial[(long long)blockIdx.x * kGramRows * kGramCols + e] = red[e / p][e % p];
 }
 
+// Single dot product x . y (norms): every lane loads, block partial in
+// partial[blk][0], summed in block order by k_gram_finish.
+__global__ void __launch_bounds__(256)
+    k_dot(const double *__restrict__ x, const double *__restrict__ y, long long n,
+          long long chunk, double *__restrict__ partial, GramDev gd) {
+    if (gd.stop && *gd.stop) return;
+    __shared__ double red[8];
+    const long long lo = (long long)blockIdx.x * chunk, hi = min(n, lo + chunk);
+    double s = 0.0;
+    for (long long k = lo + threadIdx.x; k < hi; k += 256) s += x[k] * y[k];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; w++) t += red[w];
+        partial[(long long)blockIdx.x * kGramRows * kGramCols] = t;
+    }
+}
+
 // out[e] = sum_b partial[b][e] in a fixed order (bitwise reproducible).
 __global__ void k_gram_finish(const double *__restrict__ partial, int nb, int mp, double *out,
                               GramDev gd, int p) {
@@ -312,30 +332,51 @@ __global__ void k_f2d(const float *__restrict__ in, double *__restrict__ out, lo
             out[c * ldo + k] = (double)in[c * ldi + k];
 }
 
-// Cyclic Jacobi eigensolve of the m x m symmetric matrix held in the lower
-// triangle of G (G[i*ldg + j], i >= j), one warp.  Eigenvalues ascending in
-// w; eigenvector k in Y[k*ldg + .], sign fixed so that its largest-magnitude
-// component is positive.  info = number of sweeps, or -1 if not converged.
-__global__ void k_jacobi(const double *__restrict__ G, int m, int ldg, double *w, double *Y,
-                         int *info, const DavCtl *ctl) {
+// Jacobi eigensolve of the m x m symmetric matrix held in the lower
+// triangle of G (G[i*ldg + j], i >= j), one CTA of kJacobiThreads threads.
+// Parallel cyclic Jacobi: a sweep is m'-1 rounds (m' = m rounded up to
+// even) of m'/2 disjoint rotations in round-robin order (one index fixed,
+// the others rotating), so a round applies J^T A J for all its pairs at
+// once: angles, then the column updates (with those of the eigenvector
+// matrix), then the row updates; pair j goes to warp j % 8, element k to
+// lane k % 32.  Each rotation annihilates A[p][q] with the classic angle
+// t = sign(th) / (|th| + sqrt(th^2 + 1)), th = (Aqq - App) / 2Apq.
+// Converged when the sum of squared off-diagonal entries is below 1e-30 of
+// the diagonal's.  Eigenvalues ascending in w (equal values keep their
+// index order); eigenvector k in Y[k*ldg + .], sign fixed so that its
+// largest-magnitude component is positive.  info = number of sweeps, or -1
+// if not converged in 60.
+constexpr int kJacobiThreads = 256;
+
+__global__ void __launch_bounds__(kJacobiThreads)
+    k_jacobi(const double *__restrict__ G, int m, int ldg, double *w, double *Y, int *info,
+             const DavCtl *ctl) {
     if (ctl) {
         if (ctl->stop) return;
         m = ctl->ckdim;
     }
     extern __shared__ double sm[];
+    const int st = m + 1;
     double *A = sm;                 // m x (m+1)
-    double *Vm = sm + m * (m + 1);  // m x (m+1)
-    const int lane = threadIdx.x, st = m + 1;
-    for (int i = lane; i < m * m; i += 32) {
+    double *Vm = sm + m * st;       // m x (m+1)
+    __shared__ double rc[kMaxKry / 2], rs[kMaxKry / 2];
+    __shared__ int rp[kMaxKry / 2], rq[kMaxKry / 2];
+    __shared__ double red_off[kJacobiThreads / 32], red_dia[kJacobiThreads / 32];
+    __shared__ int s_conv;
+    __shared__ int order[kMaxKry];
+    const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31;
+    const int nwarp = nt >> 5;
+    for (int i = tid; i < m * m; i += nt) {
         int r = i / m, c = i % m;
         A[r * st + c] = r >= c ? G[r * ldg + c] : G[c * ldg + r];
         Vm[r * st + c] = r == c ? 1.0 : 0.0;
     }
-    __syncwarp();
+    __syncthreads();
+    const int me = m + (m & 1), npr = me / 2;
     int sweep = 0, conv = 0;
     for (; sweep < 60; sweep++) {
         double off = 0.0, dia = 0.0;
-        for (int i = lane; i < m * m; i += 32) {
+        for (int i = tid; i < m * m; i += nt) {
             int r = i / m, c = i % m;
             double x = A[r * st + c];
             if (r != c) off += x * x;
@@ -345,64 +386,105 @@ __global__ void k_jacobi(const double *__restrict__ G, int m, int ldg, double *w
             off += __shfl_xor_sync(0xffffffffu, off, o);
             dia += __shfl_xor_sync(0xffffffffu, dia, o);
         }
-        if (off <= 1e-30 * fmax(dia, 1e-300)) {
+        if (lane == 0) {
+            red_off[warp] = off;
+            red_dia[warp] = dia;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double so = 0.0, sd = 0.0;
+            for (int k = 0; k < nwarp; k++) {
+                so += red_off[k];
+                sd += red_dia[k];
+            }
+            s_conv = so <= 1e-30 * fmax(sd, 1e-300);
+        }
+        __syncthreads();
+        if (s_conv) {
             conv = 1;
             break;
         }
-        for (int p = 0; p < m - 1; p++)
-            for (int q = p + 1; q < m; q++) {
-                double apq = A[p * st + q];
-                double app = A[p * st + p], aqq = A[q * st + q];
-                if (fabs(apq) <= 1e-300 || fabs(apq) <= 1e-18 * sqrt(fabs(app * aqq))) continue;
-                double th = (aqq - app) / (2.0 * apq);
-                double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
-                double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
-                __syncwarp();
+        for (int round = 0; round < me - 1; round++) {
+            if (tid < npr) {
+                // circle method: position 0 fixed, positions 1..me-1 rotate
+                int a = tid, b = me - 1 - tid;
+                int p = a == 0 ? 0 : (a - 1 + round) % (me - 1) + 1;
+                int q = b == 0 ? 0 : (b - 1 + round) % (me - 1) + 1;
+                if (p > q) {
+                    int x = p;
+                    p = q;
+                    q = x;
+                }
+                double c = 1.0, sn = 0.0;
+                if (q < m) {
+                    double apq = A[p * st + q], app = A[p * st + p], aqq = A[q * st + q];
+                    if (!(fabs(apq) <= 1e-300 || fabs(apq) <= 1e-18 * sqrt(fabs(app * aqq)))) {
+                        double th = (aqq - app) / (2.0 * apq);
+                        double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+                        c = 1.0 / sqrt(t * t + 1.0);
+                        sn = t * c;
+                    }
+                }
+                rp[tid] = p;
+                rq[tid] = q < m ? q : p;
+                rc[tid] = c;
+                rs[tid] = sn;
+            }
+            __syncthreads();
+            // columns p, q of A and of the eigenvector matrix
+            for (int j = warp; j < npr; j += nwarp) {
+                const double c = rc[j], sn = rs[j];
+                if (sn == 0.0) continue;
+                const int p = rp[j], q = rq[j];
                 for (int k = lane; k < m; k += 32) {
                     double akp = A[k * st + p], akq = A[k * st + q];
-                    A[k * st + p] = c * akp - s * akq;
-                    A[k * st + q] = s * akp + c * akq;
+                    A[k * st + p] = c * akp - sn * akq;
+                    A[k * st + q] = sn * akp + c * akq;
+                    double vkp = Vm[k * st + p], vkq = Vm[k * st + q];
+                    Vm[k * st + p] = c * vkp - sn * vkq;
+                    Vm[k * st + q] = sn * vkp + c * vkq;
                 }
-                __syncwarp();
+            }
+            __syncthreads();
+            // rows p, q of A
+            for (int j = warp; j < npr; j += nwarp) {
+                const double c = rc[j], sn = rs[j];
+                if (sn == 0.0) continue;
+                const int p = rp[j], q = rq[j];
                 for (int k = lane; k < m; k += 32) {
                     double apk = A[p * st + k], aqk = A[q * st + k];
-                    A[p * st + k] = c * apk - s * aqk;
-                    A[q * st + k] = s * apk + c * aqk;
-                    double vkp = Vm[k * st + p], vkq = Vm[k * st + q];
-                    Vm[k * st + p] = c * vkp - s * vkq;
-                    Vm[k * st + q] = s * vkp + c * vkq;
+                    A[p * st + k] = c * apk - sn * aqk;
+                    A[q * st + k] = sn * apk + c * aqk;
                 }
-                __syncwarp();
             }
+            __syncthreads();
+        }
     }
-    __syncwarp();
-    if (lane == 0) {
-        // selection order by eigenvalue (stable for equal values)
-        int ord[kMaxKry];
-        for (int i = 0; i < m; i++) ord[i] = i;
-        for (int i = 1; i < m; i++) {
-            int x = ord[i], j = i;
-            while (j > 0 && A[ord[j - 1] * st + ord[j - 1]] > A[x * st + x]) {
-                ord[j] = ord[j - 1];
-                j--;
+    // eigenvalue order: rank of each diagonal entry, ties by index
+    for (int i = tid; i < m; i += nt) {
+        double x = A[i * st + i];
+        int r = 0;
+        for (int j = 0; j < m; j++) {
+            double y = A[j * st + j];
+            r += (y < x) || (y == x && j < i);
+        }
+        order[r] = i;
+    }
+    __syncthreads();
+    for (int k = tid; k < m; k += nt) {
+        int c = order[k];
+        w[k] = A[c * st + c];
+        double big = 0.0;
+        int bi = 0;
+        for (int i = 0; i < m; i++)
+            if (fabs(Vm[i * st + c]) > big + 1e-14) {
+                big = fabs(Vm[i * st + c]);
+                bi = i;
             }
-            ord[j] = x;
-        }
-        for (int k = 0; k < m; k++) {
-            int c = ord[k];
-            w[k] = A[c * st + c];
-            double big = 0.0;
-            int bi = 0;
-            for (int i = 0; i < m; i++)
-                if (fabs(Vm[i * st + c]) > big + 1e-14) {
-                    big = fabs(Vm[i * st + c]);
-                    bi = i;
-                }
-            double sg = Vm[bi * st + c] < 0 ? -1.0 : 1.0;
-            for (int i = 0; i < m; i++) Y[k * ldg + i] = sg * Vm[i * st + c];
-        }
-        *info = conv ? sweep : -1;
+        double sg = Vm[bi * st + c] < 0 ? -1.0 : 1.0;
+        for (int i = 0; i < m; i++) Y[k * ldg + i] = sg * Vm[i * st + c];
     }
+    if (tid == 0) *info = conv ? sweep : -1;
 }
 
 // ---- kernels of a graph-captured iteration (one CTA, except k_it_store) ----
@@ -568,8 +650,11 @@ static jci_status gram(Ctx &c, const double *X, int m, const double *Y, int p, d
     if (m < 1 || m > kGramRows || p < 1 || p > kGramCols) return JCI_ERR_ARG;
     long long chunk = ((c.n + kDotBlocks - 1) / kDotBlocks + 63) / 64 * 64;
     int nb = (int)((c.n + chunk - 1) / chunk);
-    gram_kernel((m + 7) / 8, (p + 7) / 8)<<<nb, 256, 0, c.st>>>(X, m, Y, p, c.ld, c.n, chunk,
-                                                                 c.b->partial, gd);
+    if (m == 1 && p == 1 && !gd.mdev)
+        k_dot<<<nb, 256, 0, c.st>>>(X, Y, c.n, chunk, c.b->partial, gd);
+    else
+        gram_kernel((m + 7) / 8, (p + 7) / 8)<<<nb, 256, 0, c.st>>>(X, m, Y, p, c.ld, c.n,
+                                                                     chunk, c.b->partial, gd);
     k_gram_finish<<<m * p, 32, 0, c.st>>>(c.b->partial, nb, m * p, out, gd, p);
     JCI_CUDA(cudaGetLastError());
     return JCI_OK;
@@ -613,7 +698,8 @@ static jci_status rayleigh_ritz(Ctx &c, int m, const std::vector<double> &G,
     // the attribute is per device; setting it again is harmless and cheap
     JCI_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(2 * kMaxKry * (kMaxKry + 1) * sizeof(double))));
-    k_jacobi<<<1, 32, smem, c.st>>>(b->G, m, kMaxKry, b->eval, b->evec, c.d_info, nullptr);
+    k_jacobi<<<1, kJacobiThreads, smem, c.st>>>(b->G, m, kMaxKry, b->eval, b->evec, c.d_info,
+                                                nullptr);
     int info = 0;
     JCI_CUDA(cudaMemcpyAsync(w.data(), b->eval, m * sizeof(double), cudaMemcpyDeviceToHost, c.st));
     JCI_CUDA(cudaMemcpyAsync(Y.data(), b->evec, kMaxKry * kMaxKry * sizeof(double),
@@ -825,7 +911,7 @@ static jci_status enqueue_iteration(Ctx &c, bool fp32, int kmax) {
     k_it_store<<<g, 256, 0, c.st>>>(b->C, c.ld, 0, b->cnew, c.n, ctl);
     if ((r = gram(c, b->C, kmax, b->t, 1, b->dots, with_new))) return r;
     k_it_append<<<1, 64, 0, c.st>>>(ctl, b->dots, b->G);
-    k_jacobi<<<1, 32, 2 * (size_t)kmax * (kmax + 1) * sizeof(double), c.st>>>(
+    k_jacobi<<<1, kJacobiThreads, 2 * (size_t)kmax * (kmax + 1) * sizeof(double), c.st>>>(
         b->G, 0, kMaxKry, b->eval, b->evec, b->info, ctl);
     k_it_end<<<1, 1, 0, c.st>>>(ctl, b->info, kmax);
     JCI_CUDA(cudaGetLastError());

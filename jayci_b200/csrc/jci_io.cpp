@@ -9,7 +9,10 @@
 //    dword with four 16-bit fields most-significant first (ulab16), 8-bit
 //    orbital labels eight per word most-significant first (ulab8));
 //  * unformatted vector files civec / ci.restart / hvvec (int32 dim, int32
-//    len, dim*len float64; mpi_utilities.c:353-532).
+//    len, dim*len float64; mpi_utilities.c:353-532);
+//  * the Dyson-orbital program's dycicalc.in namelists &wavefcn0 /
+//    &wavefcn1 / &dysonorbital (readnamelist.f90:110-180, ioutil.c:154-260)
+//    and its dysonorb.dat output (run_pdycicalc.c:674-712).
 #include <cctype>
 #include <cmath>
 #include <cstdint>
@@ -475,4 +478,145 @@ extern "C" jci_status jci_read_vectors(const char *path, int dim, int len, doubl
         st = JCI_ERR_FORMAT;
     fclose(f);
     return st;
+}
+
+// ---- Dyson-orbital input and output -------------------------------------
+
+namespace {
+
+// key = value-list entries of a namelist body: "states0 = 1, 2" or
+// "states0(2) = 3" (a 1-based element).  Values run up to the next key.
+struct ListEntry {
+    std::string key;
+    int index;  // 0: whole array / scalar; else 1-based element
+    std::vector<std::string> values;
+};
+
+bool parse_lists(const std::string &body, std::vector<ListEntry> &out) {
+    std::vector<std::string> tok;
+    std::string cur;
+    for (char c : body) {
+        if (std::isspace((unsigned char)c) || c == ',') {
+            if (!cur.empty()) tok.push_back(cur);
+            cur.clear();
+        } else if (c == '=') {
+            if (!cur.empty()) tok.push_back(cur);
+            cur.clear();
+            tok.push_back("=");
+        } else {
+            cur.push_back(c);
+        }
+    }
+    if (!cur.empty()) tok.push_back(cur);
+    for (size_t i = 0; i < tok.size();) {
+        if (i + 1 >= tok.size() || tok[i + 1] != "=" || tok[i] == "=") return false;
+        ListEntry e;
+        std::string k = lower(tok[i]);
+        e.index = 0;
+        size_t lp = k.find('(');
+        if (lp != std::string::npos) {
+            size_t rp = k.find(')', lp);
+            if (rp == std::string::npos) return false;
+            e.index = atoi(k.substr(lp + 1, rp - lp - 1).c_str());
+            if (e.index < 1) return false;
+            k = k.substr(0, lp);
+        }
+        e.key = k;
+        i += 2;
+        while (i < tok.size() && tok[i] != "=" && !(i + 1 < tok.size() && tok[i + 1] == "="))
+            e.values.push_back(tok[i++]);
+        if (e.values.empty()) return false;
+        out.push_back(e);
+    }
+    return true;
+}
+
+bool read_text(const char *path, std::string &text) {
+    FILE *f = fopen(path, "rb");
+    if (!f) return false;
+    char buf[4096];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, n);
+    fclose(f);
+    return true;
+}
+
+jci_status read_wavefcn(const std::string &text, const char *name, jci_wavefcn *w) {
+    *w = jci_wavefcn{0, 0, 0, 0, 0, 0, 0, 0};
+    std::string body;
+    std::vector<ListEntry> kv;
+    if (!namelist_body(text, name, body) || !parse_lists(body, kv)) return JCI_ERR_FORMAT;
+    for (auto &e : kv) {
+        double x;
+        if (e.index || e.values.size() != 1 || !parse_number(e.values[0], &x))
+            return JCI_ERR_FORMAT;
+        int v = (int)x;
+        if (e.key == "electrons") w->electrons = v;
+        else if (e.key == "orbitals") w->orbitals = v;
+        else if (e.key == "nfrozen") w->nfrozen = v;
+        else if (e.key == "ndocc") w->ndocc = v;
+        else if (e.key == "nactive") w->nactive = v;
+        else if (e.key == "nfrzvirt") w->nfrzvirt = v;
+        else if (e.key == "xlevel") w->xlevel = v;
+        else if (e.key == "nstates") w->nstates = v;
+        else return JCI_ERR_FORMAT;
+    }
+    return JCI_OK;
+}
+
+}  // namespace
+
+extern "C" jci_status jci_read_dycicalc(const char *path, jci_wavefcn *wf0, jci_wavefcn *wf1,
+                                        int *states0, int *nst0, int *states1, int *nst1) {
+    if (!path || !wf0 || !wf1 || !states0 || !nst0 || !states1 || !nst1) return JCI_ERR_ARG;
+    std::string text;
+    if (!read_text(path, text)) return JCI_ERR_IO;
+    jci_status r;
+    if ((r = read_wavefcn(text, "wavefcn0", wf0))) return r;
+    if ((r = read_wavefcn(text, "wavefcn1", wf1))) return r;
+    // readnamelist.f90:164-165 defaults
+    int s[2][5] = {{1, 0, 0, 0, 0}, {1, 0, 0, 0, 0}};
+    std::string body;
+    std::vector<ListEntry> kv;
+    if (!namelist_body(text, "dysonorbital", body) || !parse_lists(body, kv))
+        return JCI_ERR_FORMAT;
+    for (auto &e : kv) {
+        int w = e.key == "states0" ? 0 : e.key == "states1" ? 1 : -1;
+        if (w < 0) return JCI_ERR_FORMAT;
+        int first = e.index ? e.index - 1 : 0;
+        if (first + (int)e.values.size() > 5) return JCI_ERR_FORMAT;
+        for (size_t i = 0; i < e.values.size(); i++) {
+            double x;
+            if (!parse_number(e.values[i], &x)) return JCI_ERR_FORMAT;
+            s[w][first + i] = (int)x;
+        }
+    }
+    // ioutil.c:170-177: the count is the position of the last nonzero state
+    *nst0 = *nst1 = 0;
+    for (int i = 0; i < 5; i++) {
+        states0[i] = s[0][i];
+        states1[i] = s[1][i];
+        if (s[0][i] != 0) *nst0 = i + 1;
+        if (s[1][i] != 0) *nst1 = i + 1;
+    }
+    return JCI_OK;
+}
+
+extern "C" jci_status jci_write_dysonorb(const char *path, int ndyorbs, int orbs,
+                                         const double *dyorb, const int *states0, int nst0,
+                                         const int *states1, int nst1) {
+    if (!path || !dyorb || !states0 || !states1 || ndyorbs < 0 || orbs < 0) return JCI_ERR_ARG;
+    FILE *f = fopen(path, "w");
+    if (!f) return JCI_ERR_IO;
+    fprintf(f, " %d %d %d\n", ndyorbs, nst0, nst1);
+    fprintf(f, " %d\n", orbs);
+    for (int i = 0; i < nst0; i++) fprintf(f, " %d", states0[i]);
+    fprintf(f, "\n");
+    for (int i = 0; i < nst1; i++) fprintf(f, " %d", states1[i]);
+    fprintf(f, "\n");
+    for (int i = 0; i < ndyorbs; i++) {
+        for (int j = 0; j < orbs; j++) fprintf(f, "%15.8f\n", dyorb[(size_t)i * orbs + j]);
+        fprintf(f, "\n");
+    }
+    return fclose(f) == 0 ? JCI_OK : JCI_ERR_IO;
 }

@@ -493,6 +493,38 @@ static long long det_index(const jo_space *s, int p, int q)
                (q - s->sp[1].g[gq].start);
 }
 
+void jo_dyson(const jo_space *s0, const jo_space *s1, int nelec0, int norbs0,
+              const double *v0, const double *v1, int nst0, const int *states0,
+              int nst1, const int *states1, double *dyorb)
+{
+        const int sp = nelec0 % 2 == 0 ? 1 : 0;  /* spin that loses the electron */
+        const int ne0 = s0->sp[sp].nelec;
+        int o[JO_MAXE], r[JO_MAXE];
+        memset(dyorb, 0, sizeof(double) * nst0 * nst1 * norbs0);
+        for (long long i = 0; i < s0->ndets; i++) {
+                int pp, p, q;
+                det_strings(s0, i, &pp, &p, &q);
+                int x = sp ? q : p;
+                memcpy(o, s0->sp[sp].istr + (long long)x * ne0, sizeof(int) * ne0);
+                for (int e = 0; e < ne0; e++) {
+                        int n = 0;
+                        for (int f = 0; f < ne0; f++)
+                                if (f != e) r[n++] = o[f];
+                        int y = jo_string_index(s1, sp, r);
+                        if (y < 0) continue;
+                        long long J = sp ? det_index(s1, p, y) : det_index(s1, y, q);
+                        if (J < 0) continue;
+                        for (int j = 0; j < nst0; j++)
+                                for (int k = 0; k < nst1; k++)
+                                        dyorb[(j * nst1 + k) * norbs0 + o[e] - 1] +=
+                                            v0[(states0[j] - 1) * s0->ndets + i] *
+                                            v1[(states1[k] - 1) * s1->ndets + J];
+                }
+        }
+        double pref = sqrt((double)nelec0);
+        for (int i = 0; i < nst0 * nst1 * norbs0; i++) dyorb[i] *= pref;
+}
+
 void jo_hdiag(const jo_space *s, const double *m1, const double *m2,
               double *out)
 {

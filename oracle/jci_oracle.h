@@ -63,6 +63,18 @@ int jo_davidson(const jo_space *s, const double *m1, const double *m2,
                 int nroots, int prediagr, int refdim, double restol,
                 const double *init, double *energies, double *civec);
 
+/* Dyson orbitals between an (N+1)-electron space s0 and an N-electron
+ * space s1 (run_pdycicalc.c:392-414, dysoncomp.c:103-345): for every
+ * determinant of s0 and every electron of the spin whose count differs
+ * (beta when nelec0 is even, else alpha), remove it; when the resulting
+ * string and determinant exist in s1,
+ *   dyorb[(j*nst1 + k)*norbs0 + orbital-1] += v0[state0_j][I] v1[state1_k][J]
+ * with the other spin's string unchanged and no phase factor, then scale
+ * by sqrt(nelec0).  states are 1-based; v0 / v1 are state-major. */
+void jo_dyson(const jo_space *s0, const jo_space *s1, int nelec0, int norbs0,
+              const double *v0, const double *v1, int nst0, const int *states0,
+              int nst1, const int *states1, double *dyorb);
+
 /* Cyclic Jacobi eigensolver: a (n x n, row-major, symmetric, destroyed);
  * eigenvalues ascending in w, eigenvector k in row k of z. */
 void jo_symeig(int n, double *a, double *w, double *z);

@@ -153,6 +153,53 @@ class OracleSpace:
         return e, civ, it
 
 
+def ci_space(general):
+    """OracleSpace of a &general / &wavefcn tuple (electrons, orbitals,
+    nfrozen, ndocc, nactive, nfrzvirt, xlevel), with the reference's alpha /
+    beta split (abecalc.c: alpha takes the odd electron)."""
+    e, o, nfc, nd, na, nfv, x = general
+    ci_e = e - 2 * nfc
+    return OracleSpace((ci_e + 1) // 2, ci_e // 2, o - nfc - nfv, nd, na, x)
+
+
+def dyson(general0, general1, v0, v1, states0, states1):
+    """Dyson orbitals of the restatement (jo_dyson): (len(states0) *
+    len(states1)) x orbitals0, states 1-based."""
+    s0, s1 = ci_space(general0), ci_space(general1)
+    lib = OracleSpace.lib()
+    lib.jo_dyson.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                             ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    v0 = np.ascontiguousarray(v0, np.float64)
+    v1 = np.ascontiguousarray(v1, np.float64)
+    st0 = np.asarray(states0, np.int32)
+    st1 = np.asarray(states1, np.int32)
+    out = np.zeros((len(st0) * len(st1), general0[1]))
+    lib.jo_dyson(s0.h, s1.h, general0[0], general0[1], _ptr(v0), _ptr(v1), len(st0), _ptr(st0),
+                 len(st1), _ptr(st1), _ptr(out))
+    return out
+
+
+def ref_dyson(general0, general1, v0, v1, states0, states1):
+    """Dyson orbitals of the reference's own dysoncomp.c (oracle/_ref)."""
+    lib = RefSpace.lib()
+    lib.ref_dyson.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                              ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                              ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    g0 = np.asarray(general0, np.int32)
+    g1 = np.asarray(general1, np.int32)
+    v0 = np.ascontiguousarray(v0, np.float64)
+    v1 = np.ascontiguousarray(v1, np.float64)
+    st0 = np.asarray(states0, np.int32)
+    st1 = np.asarray(states1, np.int32)
+    out = np.zeros((len(st0) * len(st1), general0[1]))
+    r = lib.ref_dyson(_ptr(g0), _ptr(g1), v0.shape[0], _ptr(v0), v1.shape[0], _ptr(v1),
+                      len(st0), _ptr(st0), len(st1), _ptr(st1), _ptr(out))
+    if r:
+        raise ValueError(f"reference dyson failed: {r}")
+    return out
+
+
 def symeig(a):
     a = np.array(a, float, order="C")
     n = a.shape[0]

@@ -4,8 +4,9 @@ Runs the reference's own mpi_source C code (oracle/_ref/libjayci_ref.so,
 built from the read-only reference tree by ``make -C oracle``) single-rank
 and single-threaded on seeded synthetic integrals, and stores what it
 produces: string lists, group tables, (p,q) pairs, determinant triples,
-yij/cij tables, excitation lists, <i|H|i>, sigma on seeded random vectors
-and Davidson energies / vectors.
+yij/cij tables, excitation lists, <i|H|i>, sigma on seeded random vectors,
+Davidson energies / vectors, and Dyson orbitals between (N+1)- and
+N-electron wavefunctions.
 
     OMP_NUM_THREADS=1 python tests/golden/make_golden.py
 
@@ -101,6 +102,37 @@ def make(name):
     print(name, ref.ndets, out.get("energies"))
 
 
+# Dyson orbitals (run_pdycicalc.c / dysoncomp.c): (N+1) and N electron
+# wavefunctions on the same orbitals and integrals, their lowest states from
+# the reference's pdavidson, and the reference's Dyson orbitals.
+# name: (&wavefcn0, &wavefcn1, nstates0, nstates1, states0, states1, rank, seed)
+DYSON_CASES = {
+    # anion doublet 7e/6o (alpha electrons compared) -> neutral 6e/6o
+    "dyson_cas7_6": ((7, 6, 0, 0, 6, 0, 0), (6, 6, 0, 0, 6, 0, 0), 2, 3, [1], [1, 2], 6, 31),
+    # 8e -> 7e (beta electrons compared), DOCC/ACTV/VIRT excitation level 2
+    "dyson_trunc8_8_x2": ((8, 8, 0, 2, 4, 0, 2), (7, 8, 0, 2, 4, 0, 2), 2, 2, [1, 2], [1, 2],
+                          8, 32),
+}
+
+
+def make_dyson(name):
+    from oracle.oracle import ref_dyson
+    g0, g1, n0, n1, st0, st1, rank, seed = DYSON_CASES[name]
+    ints = make_integrals(g0[1] - g0[2] - g0[5], rank, seed)
+    m1, m2 = ints.packed()
+    vecs = []
+    for g, n in ((g0, n0), (g1, n1)):
+        ref = RefSpace(*g)
+        civ, _ = ref.davidson(m1, m2, ints.e_nuc, 0.0, maxiter=500, krymin=max(4, n),
+                              krymax=12, nroots=n, prediagr=1, refdim=8, restol=1e-9)
+        vecs.append(civ)
+    dy = ref_dyson(g0, g1, vecs[0], vecs[1], st0, st1)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), general0=np.array(g0),
+                        general1=np.array(g1), v0=vecs[0], v1=vecs[1],
+                        states0=np.array(st0), states1=np.array(st1), dyorb=dy)
+    print(name, vecs[0].shape, vecs[1].shape, np.abs(dy).max())
+
+
 if __name__ == "__main__":
-    for n in (sys.argv[1:] or CASES):
-        make(n)
+    for n in (sys.argv[1:] or list(CASES) + list(DYSON_CASES)):
+        (make_dyson if n in DYSON_CASES else make)(n)
