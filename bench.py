@@ -339,10 +339,12 @@ def run_gpu(a):
                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                       "l2": "flushed (256 MiB write) before every step",
                       "sigma_plan": {"mode": ["staged rows", "dense product, global panel",
-                                              "dense product, shared-memory panel"][mode],
-                                     "row_kernel_threads": nt,
+                                              "dense product, shared-memory panel",
+                                              "row streams on C and C^T, dense product"][mode],
+                                     ("alpha_pass_threads" if mode == 3
+                                      else "row_kernel_threads"): nt,
                                      ("staged_rows" if mode == 0 else "product_ctas_per_sm"): R,
-                                     "rows_per_cta": B}},
+                                     ("beta_pass_threads" if mode == 3 else "rows_per_cta"): B}},
            "roofline": roof, "cpu_baseline": cpu,
            "e2e": {"value": e2e, "unit": "Gdet/s", "h2d_bytes_per_step": nvec * N * 8,
                    "d2h_bytes_per_step": nvec * N * 8},

@@ -346,11 +346,18 @@ __global__ void k_f2d(const float *__restrict__ in, double *__restrict__ out, lo
 // index order); eigenvector k in Y[k*ldg + .], sign fixed so that its
 // largest-magnitude component is positive.  info = number of sweeps, or -1
 // if not converged in 60.
+//
+// With arrow set, w / Y hold on entry the eigenpairs of the leading
+// (m-1) x (m-1) block of G (the previous Rayleigh-Ritz step, before a row
+// was appended).  The sweeps then start from Q^T G Q with Q = diag(Y^T, 1):
+// diag(w) bordered by the new row Y g and G[m-1][m-1] (an arrowhead matrix),
+// with the eigenvector matrix started at Q, which takes a few sweeps instead
+// of a full diagonalisation.
 constexpr int kJacobiThreads = 256;
 
 __global__ void __launch_bounds__(kJacobiThreads)
     k_jacobi(const double *__restrict__ G, int m, int ldg, double *w, double *Y, int *info,
-             const DavCtl *ctl) {
+             const DavCtl *ctl, int arrow) {
     if (ctl) {
         if (ctl->stop) return;
         m = ctl->ckdim;
@@ -366,10 +373,27 @@ __global__ void __launch_bounds__(kJacobiThreads)
     __shared__ int order[kMaxKry];
     const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31;
     const int nwarp = nt >> 5;
-    for (int i = tid; i < m * m; i += nt) {
-        int r = i / m, c = i % m;
-        A[r * st + c] = r >= c ? G[r * ldg + c] : G[c * ldg + r];
-        Vm[r * st + c] = r == c ? 1.0 : 0.0;
+    if (arrow && m > 1) {
+        const int p = m - 1;
+        for (int i = tid; i < m * m; i += nt) {
+            int r = i / m, c = i % m;
+            A[r * st + c] = r == c && r < p ? w[r] : 0.0;
+            Vm[r * st + c] = r < p && c < p ? Y[c * ldg + r] : (r == c ? 1.0 : 0.0);
+        }
+        __syncthreads();
+        for (int k = tid; k < p; k += nt) {
+            double x = 0.0;
+            for (int i = 0; i < p; i++) x += Y[k * ldg + i] * G[p * ldg + i];
+            A[k * st + p] = x;
+            A[p * st + k] = x;
+        }
+        if (tid == 0) A[p * st + p] = G[p * ldg + p];
+    } else {
+        for (int i = tid; i < m * m; i += nt) {
+            int r = i / m, c = i % m;
+            A[r * st + c] = r >= c ? G[r * ldg + c] : G[c * ldg + r];
+            Vm[r * st + c] = r == c ? 1.0 : 0.0;
+        }
     }
     __syncthreads();
     const int me = m + (m & 1), npr = me / 2;
@@ -689,8 +713,11 @@ static jci_status gram_rows(Ctx &c, int r0, int r1, std::vector<double> &G) {
     return JCI_OK;
 }
 
+// arrow: the device eigenpairs are those of the leading (m-1) block of G
+// (the previous step of the same basis), see k_jacobi
 static jci_status rayleigh_ritz(Ctx &c, int m, const std::vector<double> &G,
-                                std::vector<double> &w, std::vector<double> &Y) {
+                                std::vector<double> &w, std::vector<double> &Y,
+                                bool arrow = false) {
     DavidsonBuffers *b = c.b;
     JCI_CUDA(cudaMemcpyAsync(b->G, G.data(), kMaxKry * kMaxKry * sizeof(double),
                              cudaMemcpyHostToDevice, c.st));
@@ -699,7 +726,7 @@ static jci_status rayleigh_ritz(Ctx &c, int m, const std::vector<double> &G,
     JCI_CUDA(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(2 * kMaxKry * (kMaxKry + 1) * sizeof(double))));
     k_jacobi<<<1, kJacobiThreads, smem, c.st>>>(b->G, m, kMaxKry, b->eval, b->evec, c.d_info,
-                                                nullptr);
+                                                nullptr, arrow ? 1 : 0);
     int info = 0;
     JCI_CUDA(cudaMemcpyAsync(w.data(), b->eval, m * sizeof(double), cudaMemcpyDeviceToHost, c.st));
     JCI_CUDA(cudaMemcpyAsync(Y.data(), b->evec, kMaxKry * kMaxKry * sizeof(double),
@@ -873,7 +900,7 @@ static jci_status host_iteration(Ctx &c, const jci_davidson_opts *o, bool fp32, 
     if ((r = sigma_block(c, ckdim, 1, fp32))) return r;
     ckdim++;
     if ((r = gram_rows(c, ckdim - 1, ckdim, G))) return r;
-    if ((r = rayleigh_ritz(c, ckdim, G, w, Y))) return r;
+    if ((r = rayleigh_ritz(c, ckdim, G, w, Y, true))) return r;
     citer++;
     *event = ckdim >= o->krymax ? 2 : 0;
     return JCI_OK;
@@ -912,7 +939,7 @@ static jci_status enqueue_iteration(Ctx &c, bool fp32, int kmax) {
     if ((r = gram(c, b->C, kmax, b->t, 1, b->dots, with_new))) return r;
     k_it_append<<<1, 64, 0, c.st>>>(ctl, b->dots, b->G);
     k_jacobi<<<1, kJacobiThreads, 2 * (size_t)kmax * (kmax + 1) * sizeof(double), c.st>>>(
-        b->G, 0, kMaxKry, b->eval, b->evec, b->info, ctl);
+        b->G, 0, kMaxKry, b->eval, b->evec, b->info, ctl, 1);
     k_it_end<<<1, 1, 0, c.st>>>(ctl, b->info, kmax);
     JCI_CUDA(cudaGetLastError());
     return JCI_OK;

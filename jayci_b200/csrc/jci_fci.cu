@@ -53,6 +53,7 @@ struct FciTables {
     int mix_grid[2] = {0, 0};      // resident CTAs of k_sigma_mixed
     int mix_occ[2] = {1, 1}, nsm = 0;
     void *tbuf[2] = {nullptr, nullptr};  // per-CTA product panels
+    void *sbuf[2] = {nullptr, nullptr};  // streaming plan: C^T and the beta part (2 N)
     uint32_t *sortB = nullptr;     // [Ib][f] beta singles sorted by target
 };
 
@@ -70,6 +71,7 @@ void fci_free(DeviceState *d) {
         cudaFree(f->d[s].a1T); cudaFree(f->d[s].joccT); cudaFree(f->d[s].dblH);
         cudaFree(f->f[s].a1T); cudaFree(f->f[s].joccT); cudaFree(f->f[s].dblH);
         cudaFree(f->tbuf[s]);
+        cudaFree(f->sbuf[s]);
     }
     cudaFree(f->sortB);
     delete f;
@@ -636,6 +638,175 @@ __global__ void __launch_bounds__(ITEMS * RB <= 4 ? 1024 : 512)
     }
 }
 
+// ---- streaming plan (mode 3) ----------------------------------------------
+//
+// Every term whose coefficient is the same for a whole row runs as row
+// streams: the diagonal and the alpha doubles on C (rows Ia), and the beta
+// singles and doubles on the transpose C^T (rows Ib), where they play the
+// role the alpha excitations play on C.  A CTA loads its output row's
+// excitation list once into shared memory; each excitation then reads one
+// whole source row, coalesced, from L2 (the vector stays resident), and no
+// per-element excitation table is read.  The beta part is added back to
+// sigma with a tiled transpose; the alpha singles and alpha x beta doubles
+// come from k_sigma_mixed as in plan 1.  Every sigma element is still
+// summed in a fixed order.
+
+constexpr int kTile = 32;
+
+// dst[c][r] = src[r][c]  (src rows x cols); 32 x 32 tiles, block (32, 8)
+template <typename T>
+__global__ void k_transpose(const T *__restrict__ src, int rows, int cols, T *__restrict__ dst,
+                            const int *skip) {
+    if (skip && *skip) return;
+    __shared__ T tile[kTile][kTile + 1];
+    const int c0 = blockIdx.x * kTile, r0 = blockIdx.y * kTile;
+    for (int j = threadIdx.y; j < kTile; j += 8) {
+        int r = r0 + j, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) tile[j][threadIdx.x] = src[(long long)r * cols + c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < kTile; j += 8) {
+        int c = c0 + j, r = r0 + threadIdx.x;
+        if (c < cols && r < rows) dst[(long long)c * rows + r] = tile[threadIdx.x][j];
+    }
+}
+
+// dst[r][c] += src[c][r]  (dst rows x cols, src cols x rows)
+template <typename T>
+__global__ void k_transpose_add(T *__restrict__ dst, int rows, int cols,
+                                const T *__restrict__ src, const int *skip) {
+    if (skip && *skip) return;
+    __shared__ T tile[kTile][kTile + 1];
+    const int c0 = blockIdx.x * kTile, r0 = blockIdx.y * kTile;
+    for (int j = threadIdx.y; j < kTile; j += 8) {
+        int sc = c0 + j, sr = r0 + threadIdx.x;
+        if (sc < cols && sr < rows) tile[j][threadIdx.x] = src[(long long)sc * rows + sr];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < kTile; j += 8) {
+        int r = r0 + j, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) dst[(long long)r * cols + c] += tile[threadIdx.x][j];
+    }
+}
+
+template <typename T>
+struct StreamArgs {
+    int rows, len;                // output rows x row length
+    int nd, ns;                   // doubles / singles of every row (ns = 0: none)
+    const int *dJ;                // [double][row] source row
+    const T *dH;                  // [double][row] value with phase
+    const uint32_t *fs;           // [single][row] source row | sign << 31
+    const uint16_t *fp;           // [single][row] pair index
+    const T *a1;                  // [single][row] one-body part
+    const T *jc;                  // [pair][column] Coulomb part of a single
+    const T *hd;                  // [row][column] diagonal, or null
+    const int *skip;
+};
+
+// Y[row][i] = hd[row][i] X[row][i] + sum_f dH_f X[dJ_f][i]
+//           + sum_f sign_f (a1_f + jc[pair_f][i]) X[target_f][i]
+// for the columns i of segment blockIdx.y (seg columns each), so that a
+// thread holds at most ITEMS <= 16 accumulators however long the rows are.
+template <typename T, int ITEMS>
+__global__ void __launch_bounds__(ITEMS <= 8 ? 1024 : 512)
+    k_sigma_stream(StreamArgs<T> a, int seg, const T *__restrict__ X, T *__restrict__ Y) {
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *dh = reinterpret_cast<T *>(smem_raw);               // nd
+    T *sh = dh + a.nd;                                     // ns
+    int *dj = reinterpret_cast<int *>(sh + a.ns);          // nd
+    uint32_t *se = reinterpret_cast<uint32_t *>(dj + a.nd);  // ns
+    int *sp = reinterpret_cast<int *>(se + a.ns);          // ns
+    const int row = blockIdx.x, tid = threadIdx.x, nt = blockDim.x, len = a.len;
+    const int c0 = blockIdx.y * seg, c1 = min(len, c0 + seg);
+    for (int f = tid; f < a.nd; f += nt) {
+        long long o = (long long)f * a.rows + row;
+        dh[f] = a.dH[o];
+        dj[f] = a.dJ[o];
+    }
+    for (int f = tid; f < a.ns; f += nt) {
+        long long o = (long long)f * a.rows + row;
+        sh[f] = a.a1[o];
+        se[f] = a.fs[o];
+        sp[f] = a.fp[o];
+    }
+    __syncthreads();
+    T acc[ITEMS];
+    const T *xr = X + (long long)row * len;
+#pragma unroll
+    for (int it = 0; it < ITEMS; it++) {
+        int i = c0 + tid + it * nt;
+        acc[it] = a.hd && i < c1 ? a.hd[(long long)row * len + i] * xr[i] : T(0);
+    }
+#pragma unroll 2
+    for (int f = 0; f < a.nd; f++) {
+        const T h = dh[f];
+        const T *src = X + (long long)dj[f] * len;
+#pragma unroll
+        for (int it = 0; it < ITEMS; it++) {
+            int i = c0 + tid + it * nt;
+            if (i < c1) acc[it] += h * src[i];
+        }
+    }
+    for (int f = 0; f < a.ns; f++) {
+        const uint32_t e = se[f];
+        const T h = sh[f];
+        const T *src = X + (long long)(e & 0x3fffffffu) * len;
+        const T *jr = a.jc + (long long)sp[f] * len;
+#pragma unroll
+        for (int it = 0; it < ITEMS; it++) {
+            int i = c0 + tid + it * nt;
+            if (i < c1) acc[it] += flip(h + jr[i], e >> 31) * src[i];
+        }
+    }
+    T *yr = Y + (long long)row * len;
+#pragma unroll
+    for (int it = 0; it < ITEMS; it++) {
+        int i = c0 + tid + it * nt;
+        if (i < c1) yr[i] = acc[it];
+    }
+}
+
+static size_t stream_smem(int nd, int ns, size_t w) {
+    return (size_t)nd * (w + 4) + (size_t)ns * (w + 8) + 16;
+}
+
+// Column segments per row: the fewest that keep a thread at <= 16 items
+// with up to 256 threads per CTA, <= 8 with more (register budget).
+static int stream_segment(int len, int nt) {
+    int cap = nt > 256 ? 8 : 16;
+    int nseg = (len + nt * cap - 1) / (nt * cap);
+    int seg = (len + nseg - 1) / nseg;
+    return (seg + 31) / 32 * 32;
+}
+
+template <typename T>
+static jci_status launch_stream(const StreamArgs<T> &a, int nt, const T *x, T *y,
+                                cudaStream_t st) {
+    const int seg = stream_segment(a.len, nt);
+    const int items = (seg + nt - 1) / nt;
+    dim3 grid(a.rows, (a.len + seg - 1) / seg);
+    size_t smem = stream_smem(a.nd, a.ns, sizeof(T));
+#define JCI_STREAM(IT)                                                                 \
+    if (items <= IT) {                                                                 \
+        JCI_CUDA(smem_optin(k_sigma_stream<T, IT>));                                   \
+        k_sigma_stream<T, IT><<<grid, nt, smem, st>>>(a, seg, x, y);                   \
+        return JCI_OK;                                                                 \
+    }
+    JCI_STREAM(1)
+    JCI_STREAM(2)
+    JCI_STREAM(4)
+    JCI_STREAM(8)
+    JCI_STREAM(16)
+#undef JCI_STREAM
+    return JCI_ERR_ARG;
+}
+
+static bool stream_ok(int len, int nt) {
+    return (nt == 128 || nt == 256 || nt == 512 || nt == 1024) &&
+           !(nt > 32 * ((len + 31) / 32) && nt > 128);
+}
+
 static size_t rows_smem(int nb, int npair, int da, int RB, size_t w) {
     return (size_t)RB * nb * w + (size_t)RB * npair * w + (size_t)RB * da * (w + 4) + 16;
 }
@@ -893,12 +1064,63 @@ static jci_status launch_mixed2(jci_space *s, const FciArgs<T> &fa, const T *v, 
 // One full sigma of one vector with the given plan.
 // mode 0: k_sigma_fci with R staged alpha rows.  mode 1: k_sigma_rows (nt
 // threads, B rows per CTA) then k_sigma_mixed with R CTAs per SM.
+// Scratch of the streaming plan: C^T and the beta part, N each, allocated on
+// the first use of the plan (the autotuner's trial) and kept.
+template <typename T>
+static jci_status stream_scratch(FciTables *f, T **ct, T **tau) {
+    const int prec = sizeof(T) == 8 ? 0 : 1;
+    size_t n = (size_t)f->na * f->nb;
+    if (!f->sbuf[prec]) JCI_CUDA(cudaMalloc(&f->sbuf[prec], 2 * n * sizeof(T)));
+    *ct = (T *)f->sbuf[prec];
+    *tau = *ct + n;
+    return JCI_OK;
+}
+
+// alpha pass on C (rows Ia): diagonal and alpha doubles; beta pass on C^T
+// (rows Ib): beta doubles and beta singles with the alpha string's Coulomb
+// row jocc[pair][Ia] (hmatels_1x, action_util.c:210)
+template <typename T>
+static void stream_args(const FciArgs<T> &a, StreamArgs<T> &al, StreamArgs<T> &be) {
+    al.rows = a.na; al.len = a.nb; al.nd = a.da; al.ns = 0;
+    al.dJ = a.dJA; al.dH = a.dHA; al.fs = nullptr; al.fp = nullptr; al.a1 = nullptr;
+    al.jc = nullptr; al.hd = a.hd; al.skip = a.skip;
+    be.rows = a.nb; be.len = a.na; be.nd = a.db; be.ns = a.sb;
+    be.dJ = a.dJB; be.dH = a.dHB; be.fs = a.fsB; be.fp = a.fpB; be.a1 = a.a1B;
+    be.jc = a.jA; be.hd = nullptr; be.skip = a.skip;
+}
+
+template <typename T>
+static jci_status launch_transposes(const FciTables *f, const T *v, T *ct, T *o, const T *tau,
+                                    bool add, const int *skip, cudaStream_t st) {
+    dim3 tb(kTile, 8), g((f->nb + kTile - 1) / kTile, (f->na + kTile - 1) / kTile);
+    if (add)
+        k_transpose_add<T><<<g, tb, 0, st>>>(o, f->na, f->nb, tau, skip);
+    else
+        k_transpose<T><<<g, tb, 0, st>>>(v, f->na, f->nb, ct, skip);
+    JCI_CUDA(cudaGetLastError());
+    return JCI_OK;
+}
+
 template <typename T>
 static jci_status run_plan(jci_space *s, FciArgs<T> a, int mode, int nt, int R, int B,
                            const T *v, T *o, cudaStream_t st) {
     FciTables *f = s->dev->fci;
     size_t w = sizeof(T);
     jci_status r;
+    if (mode == 3) {
+        // nt: threads of the alpha pass, B: threads of the beta pass
+        T *ct, *tau;
+        if ((r = stream_scratch<T>(f, &ct, &tau))) return r;
+        StreamArgs<T> al, be;
+        stream_args(a, al, be);
+        if ((r = launch_transposes<T>(f, v, ct, o, tau, false, a.skip, st))) return r;
+        if ((r = launch_stream<T>(be, B, ct, tau, st))) return r;
+        if ((r = launch_stream<T>(al, nt, v, o, st))) return r;
+        if ((r = launch_transposes<T>(f, v, ct, o, tau, true, a.skip, st))) return r;
+        a.do_as = 0;
+        a.R = 0;
+        return launch_mixed<T>(s, a, v, o, st, R);
+    }
     if (mode == 0) {
         a.do_as = 1;
         a.R = R;
@@ -961,8 +1183,8 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
         }
     }
     // mode 1: the two kernels are independent launches, tuned separately
-    float best1 = 1e30f;
-    int b1nt = 0, b1B = 0, b1R = 0, b1mode = 1;
+    float best1 = 1e30f, bmix1 = 1e30f;
+    int b1nt = 0, b1B = 0, b1R = 0, b1mode = 1, b3R = 1;
     if (mixed_possible(f, w)) {
         float brow = 1e30f, bmix = 1e30f;
         FciArgs<T> ar = a;
@@ -982,6 +1204,8 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
             float ms = timeit([&] { return launch_mixed<T>(s, ar, v, o, st, R); });
             if (ms < bmix) { bmix = ms; b1R = R; }
         }
+        bmix1 = bmix;
+        b3R = b1R;
         if (mixed2_possible(f, w))
             for (int R : {1, 2}) {
                 float ms = timeit([&] { return launch_mixed2<T>(s, ar, v, o, st, R); });
@@ -990,18 +1214,50 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
         if (b1nt) best1 = brow + bmix;
         b1mode = bmode;
     }
+    // mode 3: streaming passes on C and C^T, the transposes, the product
+    float best3 = 1e30f;
+    int b3a = 0, b3b = 0;
+    if (mixed_possible(f, w) && bmix1 < 1e30f) {
+        T *ct = nullptr, *tau = nullptr;
+        if (!err) err = stream_scratch<T>(f, &ct, &tau);
+        StreamArgs<T> al, be;
+        stream_args(a, al, be);
+        float ba = 1e30f, bb = 1e30f;
+        for (int nt : nts) {
+            if (stream_ok(f->nb, nt) && stream_smem(al.nd, al.ns, w) <= f->smem_max) {
+                float ms = timeit([&] { return launch_stream<T>(al, nt, v, o, st); });
+                if (ms < ba) { ba = ms; b3a = nt; }
+            }
+            if (stream_ok(f->na, nt) && stream_smem(be.nd, be.ns, w) <= f->smem_max) {
+                float ms = timeit([&] { return launch_stream<T>(be, nt, ct, tau, st); });
+                if (ms < bb) { bb = ms; b3b = nt; }
+            }
+        }
+        float tt = timeit([&] {
+            jci_status q = launch_transposes<T>(f, v, ct, o, tau, false, nullptr, st);
+            return q ? q : launch_transposes<T>(f, v, ct, o, tau, true, nullptr, st);
+        });
+        if (b3a && b3b) best3 = ba + bb + tt + bmix1;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(v);
     cudaFree(o);
     if (err) return err;
-    if (!b0nt && !b1nt) return JCI_ERR_SPACE;
-    bool use1 = b1nt && best1 < best0;
-    f->tuned_mode[prec] = use1 ? b1mode : 0;
-    f->tuned_nt[prec] = use1 ? b1nt : b0nt;
-    f->tuned_R[prec] = use1 ? b1R : b0R;
-    f->tuned_B[prec] = use1 ? b1B : 1;
-    f->tuned_ms[prec] = use1 ? best1 : best0;
+    if (!b0nt && !b1nt && !(b3a && b3b)) return JCI_ERR_SPACE;
+    int mode = 0;
+    float best = best0;
+    if (b1nt && best1 < best) { mode = b1mode; best = best1; }
+    if (b3a && b3b && best3 < best) { mode = 3; best = best3; }
+    f->tuned_mode[prec] = mode;
+    f->tuned_nt[prec] = mode == 3 ? b3a : mode ? b1nt : b0nt;
+    f->tuned_R[prec] = mode == 3 ? b3R : mode ? b1R : b0R;
+    f->tuned_B[prec] = mode == 3 ? b3b : mode ? b1B : 1;
+    f->tuned_ms[prec] = best;
+    if (mode != 3 && f->sbuf[prec]) {  // the streaming scratch is not needed
+        cudaFree(f->sbuf[prec]);
+        f->sbuf[prec] = nullptr;
+    }
     return JCI_OK;
 }
 
@@ -1063,14 +1319,20 @@ jci_status fci_sigma(jci_space *s, int nvec, const void *v, void *sig, long long
     return launch_fci<double>(s, nvec, (const double *)v, (double *)sig, ld, st);
 }
 
-// Force a plan (mode 0: staged rows R, mode 1: dense product) for tests and
-// measurements; nt = threads per CTA of the row kernel.
+// Force a plan (mode 0: staged rows R, modes 1-2: dense product, mode 3:
+// row streams on C and C^T plus the dense product) for tests and
+// measurements; nt = threads per CTA of the row kernel (mode 3: alpha pass,
+// B = threads of the beta pass).
 jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, int B) {
     FciTables *f = s->dev ? s->dev->fci : nullptr;
     if (!f) return JCI_ERR_STATE;
     int p = precision == JCI_FP32 ? 1 : 0;
     size_t w = p ? sizeof(float) : sizeof(double);
-    if (mode == 1 || mode == 2) {
+    if (mode == 3) {
+        if (!mixed_possible(f, w) || !stream_ok(f->nb, nt) || !stream_ok(f->na, B) || R < 0 ||
+            stream_smem(f->da, 0, w) > f->smem_max || stream_smem(f->db, f->sb, w) > f->smem_max)
+            return JCI_ERR_ARG;
+    } else if (mode == 1 || mode == 2) {
         bool ok = mode == 1 ? mixed_possible(f, w) : mixed2_possible(f, w);
         if (!ok || !rows_ok(f->nb, nt, B) || R < 0 ||
             rows_smem(f->nb, f->npair, f->da, B, w) > f->smem_max)

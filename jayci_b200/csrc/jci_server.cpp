@@ -67,7 +67,7 @@ size_t estimate_footprint(const jci_space *s, const jci_request &r) {
     long long n = s->ndets, ld = (n + 31) / 32 * 32;
     size_t b = 8ull * ld * (3ull * r.krymax + 2);
     if (r.precision == JCI_MIXED) b += 8ull * ld * std::max(r.krymin, r.nroots);
-    b += 12ull * n + 16ull * ld;  // hdiag (FP64+FP32), autotune scratch
+    b += 12ull * n + 32ull * ld;  // hdiag (FP64+FP32), autotune and streaming scratch
     long long npair = (long long)s->ci_orbs * (s->ci_orbs + 1) / 2;
     for (int sp = 0; sp < 2; sp++) {
         const SpinSpace &x = s->sp[sp];

@@ -82,7 +82,8 @@ def test_sigma_against_oracle(gen):
 @pytest.mark.parametrize("plan", [(0, 128, 1, 1), (0, 256, 4, 1), (0, 512, 16, 1),
                                   (1, 128, 1, 1), (1, 256, 2, 2), (1, 128, 0, 4),
                                   (1, 1024, 4, 1), (1, 512, 1, 4), (2, 256, 1, 2),
-                                  (2, 512, 2, 1), (2, 128, 0, 4)])
+                                  (2, 512, 2, 1), (2, 128, 0, 4), (3, 128, 1, 128),
+                                  (3, 256, 0, 512), (3, 1024, 2, 256)])
 @pytest.mark.parametrize("prec", [jb.FP64, jb.FP32])
 def test_every_fci_plan(name, plan, prec):
     """Each launch plan the autotuner may pick gives the reference's sigma."""
