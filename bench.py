@@ -56,6 +56,23 @@ def env_int(k, d):
     return int(os.environ.get(k, d))
 
 
+def max_over_ranks(dist, values, device):
+    """Each value's maximum over all ranks (the slowest replica's time); the
+    values themselves when running alone (dist is None)."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def replica_rate(world, units_per_rank, seconds):
+    """Whole-job throughput of independent replicas: the units every rank
+    processed over the slowest rank's time (weak scaling), in units/s."""
+    return world * units_per_rank / seconds
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -258,12 +275,9 @@ def run_gpu(a):
         dist.barrier()
     clk = clocks.stop()
     tot32_ms, launches32 = timed(a.steps, jb.FP32, V32, S32)
-    if dist:
-        t = torch.tensor([tot_ms, tot32_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms, tot32_ms = float(t[0]), float(t[1])
-    value = world * N * nvec * a.steps / (tot_ms / 1e3) / 1e9
-    value32 = world * N * nvec * a.steps / (tot32_ms / 1e3) / 1e9
+    tot_ms, tot32_ms = max_over_ranks(dist, [tot_ms, tot32_ms], "cuda")
+    value = replica_rate(world, N * nvec * a.steps, tot_ms / 1e3) / 1e9
+    value32 = replica_rate(world, N * nvec * a.steps, tot32_ms / 1e3) / 1e9
 
     # end to end through the C ABI from pinned host memory
     hv = torch.randn(nvec, N, dtype=torch.float64, generator=torch.Generator().manual_seed(7))
@@ -284,11 +298,8 @@ def run_gpu(a):
             raise jb.JciError(rc, "jci_sigma")
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t[0])
-    e2e = world * N * nvec * a.steps / e2e_s / 1e9
+    e2e_s, = max_over_ranks(dist, [e2e_s], "cuda")
+    e2e = replica_rate(world, N * nvec * a.steps, e2e_s) / 1e9
 
     # roofline of the sigma kernel (row-stream algorithmic bytes per vector)
     w = 8
