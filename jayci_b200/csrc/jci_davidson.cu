@@ -155,10 +155,13 @@ __global__ void __launch_bounds__(256)
     for (int a = 0; a < MT; a++)
 #pragma unroll
         for (int b = 0; b < PT; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
-    for (long long k0 = lo + warp * 4; k0 < hi; k0 += 64) {
-        double av[2][MT], bv[2][PT];
+    // U 4-element steps per lane in flight (the same summation order for
+    // every U: steps k0, k0+32, k0+64, ...)
+    constexpr int U = MT <= 4 ? 4 : 2;
+    for (long long k0 = lo + warp * 4; k0 < hi; k0 += 32 * U) {
+        double av[U][MT], bv[U][PT];
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
+        for (int u = 0; u < U; u++) {
             const long long k = k0 + 32 * u + t;
             const bool in = k < hi;
 #pragma unroll
@@ -167,7 +170,7 @@ __global__ void __launch_bounds__(256)
             for (int b = 0; b < PT; b++) bv[u][b] = in && yv[b] ? yr[b][k] : 0.0;
         }
 #pragma unroll
-        for (int u = 0; u < 2; u++)
+        for (int u = 0; u < U; u++)
 #pragma unroll
             for (int a = 0; a < MT; a++)
 #pragma unroll

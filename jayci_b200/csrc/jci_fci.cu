@@ -1239,6 +1239,18 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
         });
         if (b3a && b3b) best3 = ba + bb + tt + bmix1;
     }
+    // the components were timed one by one; time each plan's best
+    // configuration end to end before choosing
+    auto best_of = [&](auto fn) {
+        float m = 1e30f;
+        for (int k = 0; k < 3; k++) m = std::min(m, timeit(fn));
+        return m;
+    };
+    if (b0nt) best0 = best_of([&] { return run_plan<T>(s, a, 0, b0nt, b0R, 1, v, o, st); });
+    if (b1nt)
+        best1 = best_of([&] { return run_plan<T>(s, a, b1mode, b1nt, b1R, b1B, v, o, st); });
+    if (b3a && b3b)
+        best3 = best_of([&] { return run_plan<T>(s, a, 3, b3a, b3R, b3b, v, o, st); });
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(v);
