@@ -56,6 +56,24 @@ def env_int(k, d):
     return int(os.environ.get(k, d))
 
 
+# kernels per sigma vector of each plan (jci_sigma_tuning modes)
+SIGMA_KERNELS = {0: 1, 1: 2, 2: 2, 3: 5, 4: 5, 5: 2}
+PLAN_NAMES = {0: "staged rows", 1: "row kernel, dense product through a global panel",
+              2: "row kernel, dense product from shared-memory chunks",
+              3: "row streams on C and C^T, dense product through a global panel",
+              4: "row streams on C and C^T, fused product and gather",
+              5: "row kernel, fused product and gather"}
+
+
+def sigma_plan_desc(mode, nt, R, B):
+    streams = mode in (3, 4)
+    return {"mode": mode, "name": PLAN_NAMES[mode],
+            ("alpha_pass_threads" if streams else "row_kernel_threads"): nt,
+            ("staged_rows" if mode == 0 else
+             "product_column_threads" if mode in (4, 5) else "product_ctas_per_sm"): R,
+            ("beta_pass_threads" if streams else "rows_per_cta"): B}
+
+
 def max_over_ranks(dist, values, device):
     """Each value's maximum over all ranks (the slowest replica's time); the
     values themselves when running alone (dist is None)."""
@@ -349,17 +367,11 @@ def run_gpu(a):
            "config": {"workload": a.workload, "ndets": N, "vectors_per_step": nvec,
                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                       "l2": "flushed (256 MiB write) before every step",
-                      "sigma_plan": {"mode": ["staged rows", "dense product, global panel",
-                                              "dense product, shared-memory panel",
-                                              "row streams on C and C^T, dense product"][mode],
-                                     ("alpha_pass_threads" if mode == 3
-                                      else "row_kernel_threads"): nt,
-                                     ("staged_rows" if mode == 0 else "product_ctas_per_sm"): R,
-                                     ("beta_pass_threads" if mode == 3 else "rows_per_cta"): B}},
+                      "sigma_plan": sigma_plan_desc(mode, nt, R, B)},
            "roofline": roof, "cpu_baseline": cpu,
            "e2e": {"value": e2e, "unit": "Gdet/s", "h2d_bytes_per_step": nvec * N * 8,
                    "d2h_bytes_per_step": nvec * N * 8},
-           "gpu_launches": a.steps * nvec * (2 if mode >= 1 else 1),
+           "gpu_launches": a.steps * nvec * SIGMA_KERNELS[mode],
            "clocks": clk,
            "fp32_sigma_gdet_s": value32,
            "solves": solves}
@@ -535,6 +547,10 @@ def run_profile(a):
         o = torch.empty_like(v)
         sp.sigma_device(v.data_ptr(), o.data_ptr(), 1, sp.ndets, prec, st.cuda_stream)
         torch.cuda.synchronize()
+        if a.plan:
+            sp.set_sigma_plan(prec, *(int(x) for x in a.plan.split(",")))
+            sp.sigma_device(v.data_ptr(), o.data_ptr(), 1, sp.ndets, prec, st.cuda_stream)
+            torch.cuda.synchronize()
         if a.profile_davidson:
             # a few Davidson iterations: subspace products (k_gram), residuals,
             # preconditioner and sigma as they run inside a solve
@@ -579,6 +595,9 @@ def main():
     ap.add_argument("--profile-fp32", action="store_true")
     ap.add_argument("--profile-davidson", action="store_true",
                     help="with --profile: --steps Davidson iterations instead of sigma calls")
+    ap.add_argument("--plan", default="",
+                    help="with --profile: force the sigma plan MODE,THREADS,ROWS,BATCH "
+                         "(jci_sigma_set_plan) instead of the autotuned one")
     a = ap.parse_args()
     if a.profile:
         return run_profile(a)

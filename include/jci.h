@@ -185,30 +185,27 @@ jci_status jci_sigma_device(jci_space *s, int nvec, const void *v,
 jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sigma,
                                     int precision, void *stream);
 
-/* Plan the sigma autotuner picked for this space: mode (0 staged rows,
- * 1 dense product with a global scratch panel, 2 dense product consumed
- * from shared memory, 3 row streams on C and its transpose plus the dense
- * product), threads per CTA of the row kernel (mode 3: of the alpha pass),
- * `rows` (mode 0: alpha rows staged per pass; modes 1-3: product-kernel
- * CTAs per SM, 0 = as many as fit), `batch` (modes 1-2: alpha strings per
- * CTA of the row kernel; mode 3: threads per CTA of the beta pass), and its
- * timed cost in ms per vector.  All 0 before the first sigma call
- * and on the multi-group path.  No reference counterpart (the reference
- * has no device tuning). */
+/* Plan the sigma autotuner picked for this space: mode (0 staged rows;
+ * 1, 2, 5 a row kernel followed by the dense product through a global
+ * scratch panel (1), consumed chunk by chunk from shared memory (2), or
+ * fused with the gather over per-chunk entry lists (5); 3, 4 row streams
+ * on C and its transpose followed by the product of mode 1 (3) or of mode
+ * 5 (4)), threads per CTA of the row kernel (modes 3-4: of the alpha
+ * pass), `rows` (mode 0: alpha rows staged per pass; modes 1-3: product
+ * CTAs per SM, 0 = as many as fit; modes 4-5: column threads of the fused
+ * product, 8 or 16), `batch` (modes 1, 2, 5: alpha strings per CTA of the
+ * row kernel; modes 3-4: threads per CTA of the beta pass), and its timed
+ * cost in ms per vector.  All 0 before the first sigma call and on the
+ * multi-group path.  No reference counterpart (the reference has no device
+ * tuning). */
 jci_status jci_sigma_tuning(const jci_space *s, int precision, int *mode,
                             int *threads, int *rows, int *batch, float *ms);
 
-/* Fix the sigma plan instead of autotuning (for tests and measurements):
- * mode 0 stages `rows` alpha-excitation rows per pass in one kernel; modes
- * 1 and 2 run a row kernel with `batch` (1, 2, 4) alpha strings per CTA and
- * then the alpha singles as a dense product with `rows` CTAs per SM (0 = as
- * many as fit), through a global panel (1) or shared memory (2); mode 3
- * runs the diagonal and alpha doubles as row streams on C (`threads` per
- * CTA), the beta singles and doubles as row streams on C transposed
- * (`batch` threads per CTA) and the product of mode 1; threads =
- * 128/256/512/1024 per CTA.  Only for
- * one-group (FCI/CAS) spaces after jci_set_integrals.  No reference
- * counterpart. */
+/* Fix the sigma plan instead of autotuning (for tests and measurements),
+ * with the mode and arguments as jci_sigma_tuning reports them; threads =
+ * 128/256/512/1024 per CTA.  Only for one-group (FCI/CAS) spaces after
+ * jci_set_integrals; JCI_ERR_ARG for a plan the space cannot run.  No
+ * reference counterpart. */
 jci_status jci_sigma_set_plan(jci_space *s, int precision, int mode,
                               int threads, int rows, int batch);
 

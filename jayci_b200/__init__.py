@@ -230,9 +230,8 @@ class Space:
                                       ctypes.c_void_p(stream or 0)), "sigma_device")
 
     def sigma_tuning(self, precision=FP64):
-        """(mode, threads, rows, batch, ms per vector) chosen by the autotuner;
-        rows = staged alpha rows (mode 0) or product CTAs per SM (mode 1),
-        batch = alpha strings per CTA of the mode-1 row kernel."""
+        """(mode, threads, rows, batch, ms per vector) chosen by the autotuner,
+        with the meanings of jci_sigma_tuning (include/jci.h)."""
         m, a, b, g, c = (ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int(),
                          ctypes.c_float())
         _check(lib().jci_sigma_tuning(self.h, precision, ctypes.byref(m), ctypes.byref(a),
@@ -241,7 +240,7 @@ class Space:
         return m.value, a.value, b.value, g.value, c.value
 
     def set_sigma_plan(self, precision, mode, threads, rows=1, batch=1):
-        """Fix the FCI sigma plan (mode 0 staged rows, 1 dense product)."""
+        """Fix the FCI sigma plan (modes 0-5 of jci_sigma_set_plan)."""
         _check(lib().jci_sigma_set_plan(self.h, precision, mode, threads, rows, batch),
                "sigma_set_plan")
 

@@ -35,7 +35,7 @@
 namespace jci {
 
 constexpr int kMaxKry = 64;
-constexpr int kDotBlocks = 296;  // 2 x 148 SMs
+constexpr int kDotBlocks = 4 * 148;  // upper bound of the product grids (4 per SM)
 constexpr int kHist = kMaxKry + 2;
 
 // Control block of a graph-captured iteration of the root-sequential
@@ -105,18 +105,27 @@ void davidson_free(DeviceState *d) {
 // Tall-skinny products G = X^T Y of basis panels (X: m <= 64 vectors, Y:
 // p <= 16 vectors, each n long, vector-major with leading dimension ld) on
 // the FP64 tensor cores: mma.sync m8n8k4 with A = 8 vectors of X x 4
-// consecutive elements, B = the same 4 elements of 8 vectors of Y.  Lane
-// (g = lane/4, t = lane%4) loads element k0+t of vector 8a+g (A) and 8b+g
-// (B): each load instruction reads eight full 32-byte sectors.  Warps take
-// interleaved 4-element steps of the block's slice; their 8x8 tiles are
-// summed in warp order in shared memory, the block partials in block order
-// by k_gram_finish, so the result is bitwise reproducible.
+// elements, B = the same 4 elements of 8 vectors of Y.  Lane (g = lane/4,
+// t = lane%4) loads the element pair k+2t, k+2t+1 of vector 8a+g (A) and
+// 8b+g (B) with one 16-byte load and feeds the two elements to two MMAs, so
+// each load instruction reads 64 contiguous bytes of eight vectors, and the
+// eight warps of a block together read 512 contiguous bytes.  The warps' 8x8
+// tiles are summed in warp order in shared memory, the block partials in
+// block order by k_gram_finish, so the result is bitwise reproducible.
 constexpr int kGramRows = 64, kGramCols = 16;
 
 __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                  : "+d"(d[0]), "+d"(d[1])
                  : "d"(a), "d"(b));
+}
+
+// elements k, k+1 of row r (k even, r 16-byte aligned); zero past hi
+__device__ __forceinline__ double2 load_pair(const double *__restrict__ r, long long k,
+                                             long long hi, bool valid) {
+    if (!valid || k >= hi) return make_double2(0.0, 0.0);
+    if (k + 1 < hi) return *reinterpret_cast<const double2 *>(r + k);
+    return make_double2(r[k], 0.0);
 }
 
 // Row count taken from a graph-captured iteration's control block: m =
@@ -155,26 +164,30 @@ __global__ void __launch_bounds__(256)
     for (int a = 0; a < MT; a++)
 #pragma unroll
         for (int b = 0; b < PT; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
-    // U 4-element steps per lane in flight (the same summation order for
-    // every U: steps k0, k0+32, k0+64, ...)
-    constexpr int U = MT <= 4 ? 4 : 2;
-    for (long long k0 = lo + warp * 4; k0 < hi; k0 += 32 * U) {
-        double av[U][MT], bv[U][PT];
+    // The slice is cut into 8-element groups; group g goes to warp g % 8
+    // and each warp takes its groups in ascending order, whatever U (the
+    // groups in flight per step), so the summation order and the result are
+    // the same for every kernel shape.
+    constexpr int U = MT <= 2 ? 4 : (MT <= 4 ? 2 : 1);
+    for (long long g0 = warp; lo + 8 * g0 < hi; g0 += 8 * U) {
+        double2 av[U][MT], bv[U][PT];
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            const long long k = k0 + 32 * u + t;
-            const bool in = k < hi;
+            const long long k = lo + 8 * (g0 + 8 * u) + 2 * t;
 #pragma unroll
-            for (int a = 0; a < MT; a++) av[u][a] = in && xv[a] ? xr[a][k] : 0.0;
+            for (int a = 0; a < MT; a++) av[u][a] = load_pair(xr[a], k, hi, xv[a]);
 #pragma unroll
-            for (int b = 0; b < PT; b++) bv[u][b] = in && yv[b] ? yr[b][k] : 0.0;
+            for (int b = 0; b < PT; b++) bv[u][b] = load_pair(yr[b], k, hi, yv[b]);
         }
 #pragma unroll
         for (int u = 0; u < U; u++)
 #pragma unroll
             for (int a = 0; a < MT; a++)
 #pragma unroll
-                for (int b = 0; b < PT; b++) dmma_8x8x4(acc[a][b], av[u][a], bv[u][b]);
+                for (int b = 0; b < PT; b++) {
+                    dmma_8x8x4(acc[a][b], av[u][a].x, bv[u][b].x);
+                    dmma_8x8x4(acc[a][b], av[u][a].y, bv[u][b].y);
+                }
     }
     // accumulator layout: lane holds row g, columns 2t and 2t+1 of each tile
     for (int w = 0; w < 8; w++) {
@@ -675,9 +688,14 @@ static jci_status sigma_block(Ctx &c, int i0, int m, bool fp32) {
 static jci_status gram(Ctx &c, const double *X, int m, const double *Y, int p, double *out,
                        GramDev gd = GramDev()) {
     if (m < 1 || m > kGramRows || p < 1 || p > kGramCols) return JCI_ERR_ARG;
-    long long chunk = ((c.n + kDotBlocks - 1) / kDotBlocks + 63) / 64 * 64;
+    const bool dot = m == 1 && p == 1 && !gd.mdev;
+    // a fixed partition (kDotBlocks slices): the summation order, and so
+    // every bit of the result, is the same for every kernel shape and for
+    // graph-captured and host-driven iterations
+    const int grid = kDotBlocks;
+    long long chunk = ((c.n + grid - 1) / grid + 63) / 64 * 64;
     int nb = (int)((c.n + chunk - 1) / chunk);
-    if (m == 1 && p == 1 && !gd.mdev)
+    if (dot)
         k_dot<<<nb, 256, 0, c.st>>>(X, Y, c.n, chunk, c.b->partial, gd);
     else
         gram_kernel((m + 7) / 8, (p + 7) / 8)<<<nb, 256, 0, c.st>>>(X, m, Y, p, c.ld, c.n,

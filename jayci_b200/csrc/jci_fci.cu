@@ -42,7 +42,7 @@ struct FciSpin {
 };
 
 struct FciTables {
-    int na = 0, nb = 0, sa = 0, sb = 0, da = 0, db = 0, npair = 0;
+    int na = 0, nb = 0, sa = 0, sb = 0, da = 0, db = 0, npair = 0, nelb = 0;
     int *dblJ[2] = {nullptr, nullptr};   // [double][string] target string
     FciSpin<double> d[2];
     FciSpin<float> f[2];
@@ -55,6 +55,7 @@ struct FciTables {
     void *tbuf[2] = {nullptr, nullptr};  // per-CTA product panels
     void *sbuf[2] = {nullptr, nullptr};  // streaming plan: C^T and the beta part (2 N)
     uint32_t *sortB = nullptr;     // [Ib][f] beta singles sorted by target
+    AbTables ab[2];                // fused product's entry lists, 8 / 16 column threads
 };
 
 bool fci_supported(const jci_space *s) {
@@ -74,6 +75,8 @@ void fci_free(DeviceState *d) {
         cudaFree(f->sbuf[s]);
     }
     cudaFree(f->sortB);
+    ab_tables_free(&f->ab[0]);
+    ab_tables_free(&f->ab[1]);
     delete f;
     d->fci = nullptr;
 }
@@ -841,6 +844,7 @@ jci_status fci_prepare(jci_space *s) {
         f->sa = A.max_sing; f->sb = B.max_sing;
         f->da = A.max_doub; f->db = B.max_doub;
         f->npair = d->npair;
+        f->nelb = B.nelec;
         for (int sp = 0; sp < 2; sp++) {
             const SpinSpace &X = s->sp[sp];
             size_t n = (size_t)X.nstr;
@@ -1061,9 +1065,46 @@ static jci_status launch_mixed2(jci_space *s, const FciArgs<T> &fa, const T *v, 
     return JCI_OK;
 }
 
-// One full sigma of one vector with the given plan.
-// mode 0: k_sigma_fci with R staged alpha rows.  mode 1: k_sigma_rows (nt
-// threads, B rows per CTA) then k_sigma_mixed with R CTAs per SM.
+static bool ab_plan_possible(const FciTables *f, int tx, size_t w) {
+    const AbShape sh{f->nb, f->sa, f->sb, f->nelb, f->npair};
+    return ab_possible(sh, tx, w, f->smem_max);
+}
+
+// Entry lists of the fused product with tx column threads, built on first use
+// (not while a stream is being captured).
+static jci_status ab_tables(jci_space *s, int tx, cudaStream_t st, AbTables **out) {
+    FciTables *f = s->dev->fci;
+    AbTables &t = f->ab[tx == 16 ? 1 : 0];
+    if (!t.ent) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        JCI_CUDA(cudaStreamIsCapturing(st, &cs));
+        if (cs != cudaStreamCaptureStatusNone) return JCI_ERR_STATE;
+        jci_status r = ab_tables_build(s, f->npair, tx, &t);
+        if (r) return r;
+    }
+    *out = &t;
+    return JCI_OK;
+}
+
+// Fused product kernel (jci_fci_ab.cu) with tx column threads.
+template <typename T>
+static jci_status launch_ab(jci_space *s, const FciArgs<T> &fa, const T *v, T *o,
+                            cudaStream_t st, int tx) {
+    AbTables *t = nullptr;
+    jci_status r = ab_tables(s, tx, st, &t);
+    if (r) return r;
+    AbArgs<T> m;
+    m.na = fa.na; m.nb = fa.nb; m.sa = fa.sa; m.npair = fa.npair; m.mrows = fa.npair + 1;
+    m.nchunk = t->nchunk;
+    m.offs = t->offs;
+    m.maxent = t->maxent;
+    m.vec = (fa.nb % 2 == 0 && reinterpret_cast<uintptr_t>(v) % 16 == 0) ? 1 : 0;
+    m.fsA = fa.fsA; m.fpA = fa.fpA; m.a1A = fa.a1A; m.m2 = fa.m2;
+    m.off = t->off; m.base = t->base; m.ent = t->ent;
+    m.skip = fa.skip;
+    return ab_launch<T>(m, tx, s->dev->device, v, o, st);
+}
+
 // Scratch of the streaming plan: C^T and the beta part, N each, allocated on
 // the first use of the plan (the autotuner's trial) and kept.
 template <typename T>
@@ -1101,13 +1142,21 @@ static jci_status launch_transposes(const FciTables *f, const T *v, T *ct, T *o,
     return JCI_OK;
 }
 
+// One full sigma of one vector with the given plan.
+// mode 0: k_sigma_fci with R staged alpha rows.
+// modes 1, 2, 5: k_sigma_rows (nt threads, B rows per CTA), then the product:
+//   1: k_sigma_mixed with R CTAs per SM, 2: k_sigma_mixed2 with R CTAs per
+//   SM, 5: the fused k_sigma_ab with R column threads (8 or 16).
+// modes 3, 4: row streams on C^T (B threads) and C (nt threads), then the
+//   product: 3: k_sigma_mixed (R CTAs per SM), 4: k_sigma_ab (R column
+//   threads).
 template <typename T>
 static jci_status run_plan(jci_space *s, FciArgs<T> a, int mode, int nt, int R, int B,
                            const T *v, T *o, cudaStream_t st) {
     FciTables *f = s->dev->fci;
     size_t w = sizeof(T);
     jci_status r;
-    if (mode == 3) {
+    if (mode == 3 || mode == 4) {
         // nt: threads of the alpha pass, B: threads of the beta pass
         T *ct, *tau;
         if ((r = stream_scratch<T>(f, &ct, &tau))) return r;
@@ -1119,6 +1168,7 @@ static jci_status run_plan(jci_space *s, FciArgs<T> a, int mode, int nt, int R, 
         if ((r = launch_transposes<T>(f, v, ct, o, tau, true, a.skip, st))) return r;
         a.do_as = 0;
         a.R = 0;
+        if (mode == 4) return launch_ab<T>(s, a, v, o, st, R);
         return launch_mixed<T>(s, a, v, o, st, R);
     }
     if (mode == 0) {
@@ -1130,13 +1180,14 @@ static jci_status run_plan(jci_space *s, FciArgs<T> a, int mode, int nt, int R, 
     a.R = 0;
     if ((r = launch_rows<T>(a, nt, B, v, o, st))) return r;
     if (mode == 2) return launch_mixed2<T>(s, a, v, o, st, R);
+    if (mode == 5) return launch_ab<T>(s, a, v, o, st, R);
     return launch_mixed<T>(s, a, v, o, st, R);
 }
 
 // Pick the plan for this space by timing the admissible candidates on
-// scratch vectors: mode 0 stages R alpha rows per pass in one kernel, mode 1
-// runs the alpha singles as the dense product above; nt = threads per CTA
-// of the row kernel.  Cached per precision.
+// scratch vectors (modes as in run_plan).  The row kernel, the stream passes
+// and the product kernels are tuned one by one; the best configuration of
+// each plan is then timed end to end.  Cached per precision.
 template <typename T>
 static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     DeviceState *d = s->dev;
@@ -1182,14 +1233,42 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
             if (ms < best0) { best0 = ms; b0nt = nt; b0R = R; }
         }
     }
-    // mode 1: the two kernels are independent launches, tuned separately
-    float best1 = 1e30f, bmix1 = 1e30f;
-    int b1nt = 0, b1B = 0, b1R = 0, b1mode = 1, b3R = 1;
-    if (mixed_possible(f, w)) {
-        float brow = 1e30f, bmix = 1e30f;
-        FciArgs<T> ar = a;
-        ar.do_as = 0;
-        ar.R = 0;
+    // the product kernels (alpha singles, alpha x beta doubles), tuned on
+    // their own: panel (R CTAs per SM), panel-free chunks, fused (tx)
+    FciArgs<T> ar = a;
+    ar.do_as = 0;
+    ar.R = 0;
+    float bpanel = 1e30f, bmix2 = 1e30f, bab = 1e30f;
+    int Rpanel = 1, Rmix2 = 1, txab = 0;
+    if (mixed_possible(f, w))
+        for (int R : {1, 2, 4}) {
+            float ms = timeit([&] { return launch_mixed<T>(s, ar, v, o, st, R); });
+            if (ms < bpanel) { bpanel = ms; Rpanel = R; }
+        }
+    if (mixed2_possible(f, w))
+        for (int R : {1, 2}) {
+            float ms = timeit([&] { return launch_mixed2<T>(s, ar, v, o, st, R); });
+            if (ms < bmix2) { bmix2 = ms; Rmix2 = R; }
+        }
+    for (int tx : {8, 16}) {
+        if (!ab_plan_possible(f, tx, w)) continue;
+        float ms = timeit([&] { return launch_ab<T>(s, ar, v, o, st, tx); });
+        if (ms < bab) { bab = ms; txab = tx; }
+    }
+    // best product behind the row kernel (modes 1, 2, 5) and behind the
+    // stream passes (modes 3, 4)
+    float bprod = bpanel;
+    int pmode = 1, pR = Rpanel;
+    if (bmix2 < bprod) { bprod = bmix2; pmode = 2; pR = Rmix2; }
+    if (bab < bprod) { bprod = bab; pmode = 5; pR = txab; }
+    const bool sab = bab < bpanel;
+    const float bsprod = sab ? bab : bpanel;
+    const int smode = sab ? 4 : 3, sR = sab ? txab : Rpanel;
+    // modes 1, 2, 5: the row kernel, then the product
+    float best1 = 1e30f;
+    int b1nt = 0, b1B = 0, b1R = pR, b1mode = pmode;
+    if (bprod < 1e30f) {
+        float brow = 1e30f;
         for (int nt : nts) {
             if (!useful(nt)) continue;
             for (int B : {1, 2, 4}) {
@@ -1199,25 +1278,12 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
                 if (ms < brow) { brow = ms; b1nt = nt; b1B = B; }
             }
         }
-        int bmode = 1;
-        for (int R : {1, 2, 4}) {
-            float ms = timeit([&] { return launch_mixed<T>(s, ar, v, o, st, R); });
-            if (ms < bmix) { bmix = ms; b1R = R; }
-        }
-        bmix1 = bmix;
-        b3R = b1R;
-        if (mixed2_possible(f, w))
-            for (int R : {1, 2}) {
-                float ms = timeit([&] { return launch_mixed2<T>(s, ar, v, o, st, R); });
-                if (ms < bmix) { bmix = ms; b1R = R; bmode = 2; }
-            }
-        if (b1nt) best1 = brow + bmix;
-        b1mode = bmode;
+        if (b1nt) best1 = brow + bprod;
     }
-    // mode 3: streaming passes on C and C^T, the transposes, the product
+    // modes 3, 4: streaming passes on C and C^T, the transposes, the product
     float best3 = 1e30f;
     int b3a = 0, b3b = 0;
-    if (mixed_possible(f, w) && bmix1 < 1e30f) {
+    if (bsprod < 1e30f) {
         T *ct = nullptr, *tau = nullptr;
         if (!err) err = stream_scratch<T>(f, &ct, &tau);
         StreamArgs<T> al, be;
@@ -1237,7 +1303,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
             jci_status q = launch_transposes<T>(f, v, ct, o, tau, false, nullptr, st);
             return q ? q : launch_transposes<T>(f, v, ct, o, tau, true, nullptr, st);
         });
-        if (b3a && b3b) best3 = ba + bb + tt + bmix1;
+        if (b3a && b3b) best3 = ba + bb + tt + bsprod;
     }
     // the components were timed one by one; time each plan's best
     // configuration end to end before choosing
@@ -1250,7 +1316,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     if (b1nt)
         best1 = best_of([&] { return run_plan<T>(s, a, b1mode, b1nt, b1R, b1B, v, o, st); });
     if (b3a && b3b)
-        best3 = best_of([&] { return run_plan<T>(s, a, 3, b3a, b3R, b3b, v, o, st); });
+        best3 = best_of([&] { return run_plan<T>(s, a, smode, b3a, sR, b3b, v, o, st); });
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(v);
@@ -1260,13 +1326,19 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     int mode = 0;
     float best = best0;
     if (b1nt && best1 < best) { mode = b1mode; best = best1; }
-    if (b3a && b3b && best3 < best) { mode = 3; best = best3; }
+    if (b3a && b3b && best3 < best) { mode = smode; best = best3; }
+    const bool streams = mode == 3 || mode == 4;
     f->tuned_mode[prec] = mode;
-    f->tuned_nt[prec] = mode == 3 ? b3a : mode ? b1nt : b0nt;
-    f->tuned_R[prec] = mode == 3 ? b3R : mode ? b1R : b0R;
-    f->tuned_B[prec] = mode == 3 ? b3b : mode ? b1B : 1;
+    f->tuned_nt[prec] = streams ? b3a : mode ? b1nt : b0nt;
+    f->tuned_R[prec] = streams ? sR : mode ? b1R : b0R;
+    f->tuned_B[prec] = streams ? b3b : mode ? b1B : 1;
     f->tuned_ms[prec] = best;
-    if (mode != 3 && f->sbuf[prec]) {  // the streaming scratch is not needed
+    if (mode != 1 && mode != 3 && f->tbuf[prec]) {  // the product panels are not needed
+        cudaFree(f->tbuf[prec]);
+        f->tbuf[prec] = nullptr;
+        f->mix_grid[prec] = 0;
+    }
+    if (!streams && f->sbuf[prec]) {  // the streaming scratch is not needed
         cudaFree(f->sbuf[prec]);
         f->sbuf[prec] = nullptr;
     }
@@ -1331,23 +1403,24 @@ jci_status fci_sigma(jci_space *s, int nvec, const void *v, void *sig, long long
     return launch_fci<double>(s, nvec, (const double *)v, (double *)sig, ld, st);
 }
 
-// Force a plan (mode 0: staged rows R, modes 1-2: dense product, mode 3:
-// row streams on C and C^T plus the dense product) for tests and
-// measurements; nt = threads per CTA of the row kernel (mode 3: alpha pass,
-// B = threads of the beta pass).
+// Force a plan (modes as in run_plan) for tests and measurements; nt =
+// threads per CTA of the row kernel (modes 3, 4: of the alpha pass, B =
+// threads of the beta pass); R as the product kernel takes it.
 jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, int B) {
     FciTables *f = s->dev ? s->dev->fci : nullptr;
     if (!f) return JCI_ERR_STATE;
     int p = precision == JCI_FP32 ? 1 : 0;
     size_t w = p ? sizeof(float) : sizeof(double);
-    if (mode == 3) {
-        if (!mixed_possible(f, w) || !stream_ok(f->nb, nt) || !stream_ok(f->na, B) || R < 0 ||
+    if (mode == 3 || mode == 4) {
+        bool ok = mode == 3 ? mixed_possible(f, w) && R >= 0 : ab_plan_possible(f, R, w);
+        if (!ok || !stream_ok(f->nb, nt) || !stream_ok(f->na, B) ||
             stream_smem(f->da, 0, w) > f->smem_max || stream_smem(f->db, f->sb, w) > f->smem_max)
             return JCI_ERR_ARG;
-    } else if (mode == 1 || mode == 2) {
-        bool ok = mode == 1 ? mixed_possible(f, w) : mixed2_possible(f, w);
-        if (!ok || !rows_ok(f->nb, nt, B) || R < 0 ||
-            rows_smem(f->nb, f->npair, f->da, B, w) > f->smem_max)
+    } else if (mode == 1 || mode == 2 || mode == 5) {
+        bool ok = mode == 1   ? mixed_possible(f, w) && R >= 0
+                  : mode == 2 ? mixed2_possible(f, w) && R >= 0
+                              : ab_plan_possible(f, R, w);
+        if (!ok || !rows_ok(f->nb, nt, B) || rows_smem(f->nb, f->npair, f->da, B, w) > f->smem_max)
             return JCI_ERR_ARG;
     } else {
         int items = (f->nb + nt - 1) / nt;
@@ -1355,6 +1428,11 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, 
             (nt == 1024 && items > 2))
             return JCI_ERR_ARG;
         if (R < 1 || fci_smem(f->nb, f->npair, R, w) > f->smem_max) return JCI_ERR_ARG;
+    }
+    if (mode == 4 || mode == 5) {  // entry lists are built here, outside any capture
+        AbTables *t = nullptr;
+        jci_status r = ab_tables(s, R, s->dev->stream, &t);
+        if (r) return r;
     }
     f->tuned_mode[p] = mode;
     f->tuned_nt[p] = nt;

@@ -20,6 +20,38 @@ jci_status fci_sigma_noalloc(jci_space *s, const void *v, void *o, int precision
                              cudaStream_t st);
 size_t fci_noalloc_scratch_bytes();
 
+// Alpha-single x beta-single part of the one-group sigma as one fused
+// kernel (product chunks in shared memory), jci_fci_ab.cu.
+template <typename T>
+struct AbArgs {
+    int na, nb, sa, npair, mrows, nchunk;
+    int offs, maxent;       // row stride of off; longest (padded) chunk list
+    int vec;                // 16-byte copies of C rows (nb even, C 16-byte aligned)
+    const uint32_t *fsA;    // [single][Ia] target | phase << 31
+    const uint16_t *fpA;    // [single][Ia] pair index
+    const T *a1A;           // [single][Ia] one-body part
+    const T *m2;            // packed (pq|rs)
+    const uint16_t *off;    // [chunk][offs] entry offsets within the chunk
+    const uint32_t *base;   // [chunk + 1] first entry of each chunk (multiples of 4)
+    const uint32_t *ent;    // col | row << 8 | phase << 31
+    const int *skip;        // nonzero: return at once
+};
+struct AbTables {
+    int tx = 0, nchunk = 0, offs = 0, maxent = 0;
+    uint16_t *off = nullptr;
+    uint32_t *base = nullptr, *ent = nullptr;
+};
+struct AbShape {
+    int nb, sa, sb, nelb, npair;   // beta strings, singles per string, beta electrons
+};
+size_t ab_smem(const AbShape &sh, int tx, size_t w);
+bool ab_possible(const AbShape &sh, int tx, size_t w, size_t smem_max);
+jci_status ab_tables_build(const jci_space *s, int npair, int tx, AbTables *t);
+void ab_tables_free(AbTables *t);
+template <typename T>
+jci_status ab_launch(const AbArgs<T> &a, int tx, int device, const T *v, T *o,
+                     cudaStream_t st);
+
 // Generic path (any truncated space), jci_device.cu.
 jci_status device_sigma_generic(jci_space *s, int nvec, const void *vin, void *sout,
                                 long long ld, int precision, cudaStream_t st);
