@@ -57,21 +57,27 @@ def env_int(k, d):
 
 
 # kernels per sigma vector of each plan (jci_sigma_tuning modes)
-SIGMA_KERNELS = {0: 1, 1: 2, 2: 2, 3: 5, 4: 5, 5: 2}
+SIGMA_KERNELS = {0: 1, 1: 2, 2: 2, 3: 5, 4: 5, 5: 2, 6: 6, 7: 6}
 PLAN_NAMES = {0: "staged rows", 1: "row kernel, dense product through a global panel",
               2: "row kernel, dense product from shared-memory chunks",
               3: "row streams on C and C^T, dense product through a global panel",
               4: "row streams on C and C^T, fused product and gather",
-              5: "row kernel, fused product and gather"}
+              5: "row kernel, fused product and gather",
+              6: "string-group doubles, beta-singles stream, dense product through a "
+                 "global panel",
+              7: "string-group doubles, beta-singles stream, fused product and gather"}
 
 
 def sigma_plan_desc(mode, nt, R, B):
-    streams = mode in (3, 4)
-    return {"mode": mode, "name": PLAN_NAMES[mode],
-            ("alpha_pass_threads" if streams else "row_kernel_threads"): nt,
-            ("staged_rows" if mode == 0 else
-             "product_column_threads" if mode in (4, 5) else "product_ctas_per_sm"): R,
-            ("beta_pass_threads" if streams else "rows_per_cta"): B}
+    streams, groups = mode in (3, 4), mode in (6, 7)
+    d = {"mode": mode, "name": PLAN_NAMES[mode],
+         ("alpha_pass_threads" if streams else "beta_singles_threads" if groups
+          else "row_kernel_threads"): nt,
+         ("staged_rows" if mode == 0 else
+          "product_column_threads" if mode in (4, 5, 7) else "product_ctas_per_sm"): R}
+    if not groups:
+        d["beta_pass_threads" if streams else "rows_per_cta"] = B
+    return d
 
 
 def max_over_ranks(dist, values, device):

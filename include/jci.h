@@ -190,12 +190,15 @@ jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sigma,
  * scratch panel (1), consumed chunk by chunk from shared memory (2), or
  * fused with the gather over per-chunk entry lists (5); 3, 4 row streams
  * on C and its transpose followed by the product of mode 1 (3) or of mode
- * 5 (4)), threads per CTA of the row kernel (modes 3-4: of the alpha
- * pass), `rows` (mode 0: alpha rows staged per pass; modes 1-3: product
- * CTAs per SM, 0 = as many as fit; modes 4-5: column threads of the fused
+ * 5 (4); 6, 7 the same-spin doubles over groups of 16 consecutive strings,
+ * the beta singles as a row stream on the transpose, then the product of
+ * mode 1 (6) or of mode 5 (7)), threads per CTA of the row kernel (modes
+ * 3-4: of the alpha pass; modes 6-7: of the beta-singles stream), `rows`
+ * (mode 0: alpha rows staged per pass; modes 1-3 and 6: product CTAs per
+ * SM, 0 = as many as fit; modes 4, 5, 7: column threads of the fused
  * product, 8 or 16), `batch` (modes 1, 2, 5: alpha strings per CTA of the
- * row kernel; modes 3-4: threads per CTA of the beta pass), and its timed
- * cost in ms per vector.  All 0 before the first sigma call and on the
+ * row kernel; modes 3-4: threads per CTA of the beta pass; modes 6-7:
+ * unused), and its timed cost in ms per vector.  All 0 before the first sigma call and on the
  * multi-group path.  No reference counterpart (the reference has no device
  * tuning). */
 jci_status jci_sigma_tuning(const jci_space *s, int precision, int *mode,

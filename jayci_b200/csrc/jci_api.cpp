@@ -144,7 +144,7 @@ jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sig, int 
 
 jci_status jci_sigma_set_plan(jci_space *s, int precision, int mode, int threads, int rows,
                               int batch) {
-    if (!s || (precision != JCI_FP64 && precision != JCI_FP32) || mode < 0 || mode > 5)
+    if (!s || (precision != JCI_FP64 && precision != JCI_FP32) || mode < 0 || mode > 7)
         return JCI_ERR_ARG;
     if (!s->have_ints) return JCI_ERR_STATE;
     return fci_force_plan(s, precision, mode, threads, rows, batch);

@@ -56,6 +56,7 @@ struct FciTables {
     void *sbuf[2] = {nullptr, nullptr};  // streaming plan: C^T and the beta part (2 N)
     uint32_t *sortB = nullptr;     // [Ib][f] beta singles sorted by target
     AbTables ab[2];                // fused product's entry lists, 8 / 16 column threads
+    GroupTables grp[2];            // same-spin doubles by string groups, per spin
 };
 
 bool fci_supported(const jci_space *s) {
@@ -77,6 +78,8 @@ void fci_free(DeviceState *d) {
     cudaFree(f->sortB);
     ab_tables_free(&f->ab[0]);
     ab_tables_free(&f->ab[1]);
+    group_tables_free(&f->grp[0]);
+    group_tables_free(&f->grp[1]);
     delete f;
     d->fci = nullptr;
 }
@@ -888,6 +891,11 @@ jci_status fci_prepare(jci_space *s) {
             X.nstr, X.nelec, X.max_sing, X.max_doub, d->npair, t.istr, t.doub, t.a1, d->m2,
             f->d[sp].a1T, f->f[sp].a1T, f->d[sp].joccT, f->f[sp].joccT, f->dblJ[sp],
             f->d[sp].dblH, f->f[sp].dblH);
+        // the group coefficient blocks follow the current double values
+        if (f->grp[sp].uidx) {
+            jci_status r = group_fill(&f->grp[sp], f->d[sp].dblH, f->f[sp].dblH, st);
+            if (r) return r;
+        }
     }
     JCI_CUDA(cudaGetLastError());
     return JCI_OK;
@@ -1105,6 +1113,52 @@ static jci_status launch_ab(jci_space *s, const FciArgs<T> &fa, const T *v, T *o
     return ab_launch<T>(m, tx, s->dev->device, v, o, st);
 }
 
+// Group tables of both spins, built and filled on first use (not while a
+// stream is being captured).
+static jci_status group_tables(jci_space *s, cudaStream_t st) {
+    FciTables *f = s->dev->fci;
+    for (int sp = 0; sp < 2; sp++) {
+        if (f->grp[sp].uidx) continue;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        JCI_CUDA(cudaStreamIsCapturing(st, &cs));
+        if (cs != cudaStreamCaptureStatusNone) return JCI_ERR_STATE;
+        jci_status r = group_tables_build(s, sp, &f->grp[sp]);
+        if (!r) r = group_fill(&f->grp[sp], f->d[sp].dblH, f->f[sp].dblH, st);
+        if (r) {
+            group_tables_free(&f->grp[0]);
+            group_tables_free(&f->grp[1]);
+            return r;
+        }
+    }
+    return JCI_OK;
+}
+
+static bool group_possible(const FciTables *f) { return f->da >= 1 && f->db >= 1; }
+
+// Doubles of spin sp by groups: rows x len matrix x -> y (add: y += ...),
+// with the diagonal hd when given.
+template <typename T>
+static jci_status launch_group(jci_space *s, int sp, const T *hd, int add, const int *skip,
+                               const T *x, T *y, cudaStream_t st) {
+    FciTables *f = s->dev->fci;
+    jci_status r = group_tables(s, st);
+    if (r) return r;
+    const GroupTables &t = f->grp[sp];
+    GroupArgs<T> g;
+    g.rows = sp == 0 ? f->na : f->nb;
+    g.len = sp == 0 ? f->nb : f->na;
+    g.uoff = t.uoff;
+    g.uidx = t.uidx;
+    if constexpr (sizeof(T) == sizeof(double))
+        g.coef = t.c64;
+    else
+        g.coef = t.c32;
+    g.hd = hd;
+    g.add = add;
+    g.skip = skip;
+    return group_launch<T>(g, group_items(g.len, sizeof(T)), s->dev->device, x, y, st);
+}
+
 // Scratch of the streaming plan: C^T and the beta part, N each, allocated on
 // the first use of the plan (the autotuner's trial) and kept.
 template <typename T>
@@ -1150,12 +1204,31 @@ static jci_status launch_transposes(const FciTables *f, const T *v, T *ct, T *o,
 // modes 3, 4: row streams on C^T (B threads) and C (nt threads), then the
 //   product: 3: k_sigma_mixed (R CTAs per SM), 4: k_sigma_ab (R column
 //   threads).
+// modes 6, 7: the same-spin doubles by string groups on C and C^T, the beta
+//   singles as a row stream on C^T (nt threads), then the product of mode 3
+//   (6) or of mode 4 (7).
 template <typename T>
 static jci_status run_plan(jci_space *s, FciArgs<T> a, int mode, int nt, int R, int B,
                            const T *v, T *o, cudaStream_t st) {
     FciTables *f = s->dev->fci;
     size_t w = sizeof(T);
     jci_status r;
+    if (mode == 6 || mode == 7) {
+        T *ct, *tau;
+        if ((r = stream_scratch<T>(f, &ct, &tau))) return r;
+        StreamArgs<T> al, be;
+        stream_args(a, al, be);
+        be.nd = 0;  // the beta doubles come from the group kernel
+        if ((r = launch_transposes<T>(f, v, ct, o, tau, false, a.skip, st))) return r;
+        if ((r = launch_stream<T>(be, nt, ct, tau, st))) return r;
+        if ((r = launch_group<T>(s, 1, nullptr, 1, a.skip, ct, tau, st))) return r;
+        if ((r = launch_group<T>(s, 0, a.hd, 0, a.skip, v, o, st))) return r;
+        if ((r = launch_transposes<T>(f, v, ct, o, tau, true, a.skip, st))) return r;
+        a.do_as = 0;
+        a.R = 0;
+        if (mode == 7) return launch_ab<T>(s, a, v, o, st, R);
+        return launch_mixed<T>(s, a, v, o, st, R);
+    }
     if (mode == 3 || mode == 4) {
         // nt: threads of the alpha pass, B: threads of the beta pass
         T *ct, *tau;
@@ -1305,6 +1378,33 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
         });
         if (b3a && b3b) best3 = ba + bb + tt + bsprod;
     }
+    // modes 6, 7: the doubles by string groups, the beta singles as a stream
+    float best6 = 1e30f;
+    int b6s = 0;
+    if (bsprod < 1e30f && group_possible(f) && !err) {
+        T *ct = nullptr, *tau = nullptr;
+        err = stream_scratch<T>(f, &ct, &tau);
+        StreamArgs<T> al, be;
+        stream_args(a, al, be);
+        be.nd = 0;
+        float bs = 1e30f;
+        for (int nt : nts) {
+            if (!stream_ok(f->na, nt) || stream_smem(0, be.ns, w) > f->smem_max) continue;
+            float ms = timeit([&] { return launch_stream<T>(be, nt, ct, tau, st); });
+            if (ms < bs) { bs = ms; b6s = nt; }
+        }
+        float gg = timeit([&] {
+            jci_status q = launch_group<T>(s, 1, nullptr, 1, nullptr, ct, tau, st);
+            return q ? q : launch_group<T>(s, 0, a.hd, 0, nullptr, v, o, st);
+        });
+        float tt = timeit([&] {
+            jci_status q = launch_transposes<T>(f, v, ct, o, tau, false, nullptr, st);
+            return q ? q : launch_transposes<T>(f, v, ct, o, tau, true, nullptr, st);
+        });
+        if (b6s && gg < 1e30f) best6 = bs + gg + tt + bsprod;
+        err = JCI_OK;  // a space the group tables cannot hold just drops the plan
+    }
+    const int gmode = sab ? 7 : 6;
     // the components were timed one by one; time each plan's best
     // configuration end to end before choosing
     auto best_of = [&](auto fn) {
@@ -1317,28 +1417,37 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
         best1 = best_of([&] { return run_plan<T>(s, a, b1mode, b1nt, b1R, b1B, v, o, st); });
     if (b3a && b3b)
         best3 = best_of([&] { return run_plan<T>(s, a, smode, b3a, sR, b3b, v, o, st); });
+    if (best6 < 1e30f)
+        best6 = best_of([&] { return run_plan<T>(s, a, gmode, b6s, sR, 1, v, o, st); });
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(v);
     cudaFree(o);
     if (err) return err;
-    if (!b0nt && !b1nt && !(b3a && b3b)) return JCI_ERR_SPACE;
+    if (!b0nt && !b1nt && !(b3a && b3b) && best6 >= 1e30f) return JCI_ERR_SPACE;
     int mode = 0;
     float best = best0;
     if (b1nt && best1 < best) { mode = b1mode; best = best1; }
     if (b3a && b3b && best3 < best) { mode = smode; best = best3; }
-    const bool streams = mode == 3 || mode == 4;
+    if (best6 < best) { mode = gmode; best = best6; }
+    const bool streams = mode == 3 || mode == 4, groups = mode == 6 || mode == 7;
     f->tuned_mode[prec] = mode;
-    f->tuned_nt[prec] = streams ? b3a : mode ? b1nt : b0nt;
-    f->tuned_R[prec] = streams ? sR : mode ? b1R : b0R;
-    f->tuned_B[prec] = streams ? b3b : mode ? b1B : 1;
+    f->tuned_nt[prec] = groups ? b6s : streams ? b3a : mode ? b1nt : b0nt;
+    f->tuned_R[prec] = (streams || groups) ? sR : mode ? b1R : b0R;
+    f->tuned_B[prec] = groups ? 1 : streams ? b3b : mode ? b1B : 1;
     f->tuned_ms[prec] = best;
-    if (mode != 1 && mode != 3 && f->tbuf[prec]) {  // the product panels are not needed
+    // drop the group tables unless a precision uses them
+    const int other = f->tuned_mode[prec ^ 1];
+    if (!groups && other != 6 && other != 7) {
+        group_tables_free(&f->grp[0]);
+        group_tables_free(&f->grp[1]);
+    }
+    if (mode != 1 && mode != 3 && mode != 6 && f->tbuf[prec]) {  // the product panels are not needed
         cudaFree(f->tbuf[prec]);
         f->tbuf[prec] = nullptr;
         f->mix_grid[prec] = 0;
     }
-    if (!streams && f->sbuf[prec]) {  // the streaming scratch is not needed
+    if (!streams && !groups && f->sbuf[prec]) {  // the streaming scratch is not needed
         cudaFree(f->sbuf[prec]);
         f->sbuf[prec] = nullptr;
     }
@@ -1405,13 +1514,19 @@ jci_status fci_sigma(jci_space *s, int nvec, const void *v, void *sig, long long
 
 // Force a plan (modes as in run_plan) for tests and measurements; nt =
 // threads per CTA of the row kernel (modes 3, 4: of the alpha pass, B =
-// threads of the beta pass); R as the product kernel takes it.
+// threads of the beta pass; modes 6, 7: of the beta-singles stream); R as
+// the product kernel takes it.
 jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, int B) {
     FciTables *f = s->dev ? s->dev->fci : nullptr;
     if (!f) return JCI_ERR_STATE;
     int p = precision == JCI_FP32 ? 1 : 0;
     size_t w = p ? sizeof(float) : sizeof(double);
-    if (mode == 3 || mode == 4) {
+    if (mode == 6 || mode == 7) {
+        bool ok = mode == 6 ? mixed_possible(f, w) && R >= 0 : ab_plan_possible(f, R, w);
+        if (!ok || !group_possible(f) || !stream_ok(f->na, nt) ||
+            stream_smem(0, f->sb, w) > f->smem_max)
+            return JCI_ERR_ARG;
+    } else if (mode == 3 || mode == 4) {
         bool ok = mode == 3 ? mixed_possible(f, w) && R >= 0 : ab_plan_possible(f, R, w);
         if (!ok || !stream_ok(f->nb, nt) || !stream_ok(f->na, B) ||
             stream_smem(f->da, 0, w) > f->smem_max || stream_smem(f->db, f->sb, w) > f->smem_max)
@@ -1429,9 +1544,13 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, 
             return JCI_ERR_ARG;
         if (R < 1 || fci_smem(f->nb, f->npair, R, w) > f->smem_max) return JCI_ERR_ARG;
     }
-    if (mode == 4 || mode == 5) {  // entry lists are built here, outside any capture
+    if (mode == 4 || mode == 5 || mode == 7) {  // tables are built here, outside any capture
         AbTables *t = nullptr;
         jci_status r = ab_tables(s, R, s->dev->stream, &t);
+        if (r) return r;
+    }
+    if (mode == 6 || mode == 7) {
+        jci_status r = group_tables(s, s->dev->stream);
         if (r) return r;
     }
     f->tuned_mode[p] = mode;

@@ -1,0 +1,247 @@
+// jci_fci_group.cu -- same-spin doubles of the one-group sigma as a product
+// over groups of consecutive strings (hmatels_2xaa / hmatels_2xbb,
+// action_util.c).
+//
+// For output rows I in a group G of kGroupRows consecutive strings, the
+// union U_G of their double-excitation targets is listed once, and
+//   Y[I][c] = sum_{J in U_G} H[I][J] X[J][c]   (+ hd[I][c] X[I][c])
+// with H[I][J] the double's value with phase, or 0 when I does not reach J.
+// Consecutive strings share most targets (16 rows of FCI(14,14) reach 3.7x
+// fewer distinct rows than they have doubles), so every source row
+// segment is read from L2 once per group instead of once per row; the
+// zeros of the kGroupRows x |U_G| coefficient block cost FMAs, not bytes.
+// The sums run in a fixed order (U_G ascending), so results are bitwise
+// reproducible.
+#include <cuda_pipeline.h>
+
+#include <algorithm>
+#include <type_traits>
+#include <vector>
+
+#include "jci_internal.h"
+#include "jci_kernels.cuh"
+
+namespace jci {
+
+namespace {
+
+constexpr int kGroupChunk = 64;  // source rows per staged coefficient chunk
+constexpr int kGroupAhead = 8;   // source rows loaded ahead per thread
+
+// Y[I][c] for the kGroupRows rows of group blockIdx.x and the columns
+// c0 + tid + NT i (i < ITEMS) of segment blockIdx.y.
+template <typename T, int NT, int ITEMS>
+__global__ void __launch_bounds__(NT)
+    k_sigma_group(GroupArgs<T> a, const T *__restrict__ X, T *__restrict__ Y) {
+    if (a.skip && *a.skip) return;
+    constexpr int RG = kGroupRows;
+    __shared__ __align__(16) T cs[2][kGroupChunk][RG];
+    __shared__ int js[2][kGroupChunk];
+    const int g = blockIdx.x, tid = threadIdx.x, len = a.len;
+    const int r0 = g * RG, nr = min(RG, a.rows - r0);
+    const int c0 = blockIdx.y * (NT * ITEMS);
+    const long long u0 = a.uoff[g], u1 = a.uoff[g + 1];
+    auto stage = [&](long long u, int b) {
+        const int n = (int)min((long long)kGroupChunk, u1 - u);
+        // coefficient rows are RG * sizeof(T) bytes: 16-byte pieces
+        constexpr int per = RG * (int)sizeof(T) / 16;
+        for (int idx = tid; idx < n * per; idx += NT)
+            __pipeline_memcpy_async(reinterpret_cast<char *>(&cs[b][0][0]) + 16 * idx,
+                                    reinterpret_cast<const char *>(a.coef + u * RG) + 16 * idx,
+                                    16);
+        for (int idx = tid; idx < n; idx += NT) js[b][idx] = a.uidx[u + idx];
+        __pipeline_commit();
+    };
+    T acc[RG][ITEMS];
+#pragma unroll
+    for (int r = 0; r < RG; r++)
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) acc[r][i] = T(0);
+    int col[ITEMS];
+    bool in[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        col[i] = c0 + tid + NT * i;
+        in[i] = col[i] < len;
+    }
+    // one step: Q source rows loaded, then their FMAs
+    auto step = [&](int b, int k, auto qn) {
+        constexpr int Q = decltype(qn)::value;
+        T x[Q][ITEMS];
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            const T *src = X + (long long)js[b][k + q] * len;
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) x[q][i] = in[i] ? src[col[i]] : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < Q; q++) {
+            const T *h = cs[b][k + q];
+#pragma unroll
+            for (int r = 0; r < RG; r++) {
+                const T hr = h[r];
+#pragma unroll
+                for (int i = 0; i < ITEMS; i++) acc[r][i] = fma(hr, x[q][i], acc[r][i]);
+            }
+        }
+    };
+    if (u0 < u1) stage(u0, 0);
+    int b = 0;
+    for (long long u = u0; u < u1; u += kGroupChunk, b ^= 1) {
+        __pipeline_wait_prior(0);
+        __syncthreads();  // chunk b landed; every thread is done with chunk b^1
+        if (u + kGroupChunk < u1) stage(u + kGroupChunk, b ^ 1);
+        const int n = (int)min((long long)kGroupChunk, u1 - u);  // a multiple of 4
+        int k = 0;
+        for (; k + kGroupAhead <= n; k += kGroupAhead)
+            step(b, k, std::integral_constant<int, kGroupAhead>());
+        for (; k < n; k += 4) step(b, k, std::integral_constant<int, 4>());
+    }
+#pragma unroll
+    for (int r = 0; r < RG; r++) {
+        if (r < nr) {
+            const long long o = (long long)(r0 + r) * len;
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) {
+                if (!in[i]) continue;
+                T v = acc[r][i];
+                if (a.hd) v = fma(a.hd[o + col[i]], X[o + col[i]], v);
+                if (a.add) v += Y[o + col[i]];
+                Y[o + col[i]] = v;
+            }
+        }
+    }
+}
+
+// coef[(uoff[g] + upos[f][s]) RG + s - g RG] = dblH[f][s] for every double f
+// of every string s (g = s / RG); entries no double reaches stay zero.
+template <typename T>
+__global__ void k_group_coef(int nstr, int nd, const T *__restrict__ dblH,
+                             const uint16_t *__restrict__ upos, const int *__restrict__ uoff,
+                             T *__restrict__ coef) {
+    const long long n = (long long)nstr * nd;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(e % nstr), g = s / kGroupRows;
+        coef[((long long)uoff[g] + upos[e]) * kGroupRows + (s - g * kGroupRows)] = dblH[e];
+    }
+}
+
+}  // namespace
+
+// Host structure of the groups of one spin (integral-independent): the
+// sorted union of each group's double targets, padded with zero-coefficient
+// copies of its first entry to a multiple of 4, and every double's position
+// in its group's union.  The coefficients are filled on the device
+// (group_fill) from the current double values.
+jci_status group_tables_build(const jci_space *s, int spin, GroupTables *t) {
+    const SpinSpace &X = s->sp[spin];
+    const int n = X.nstr, nd = X.max_doub, ng = (n + kGroupRows - 1) / kGroupRows;
+    if (n < 1 || nd < 1) return JCI_ERR_SPACE;
+    std::vector<int> uoff(ng + 1, 0), uidx;
+    std::vector<uint16_t> upos((size_t)nd * n);
+    std::vector<int> u;
+    for (int g = 0; g < ng; g++) {
+        const int r0 = g * kGroupRows, r1 = std::min(n, r0 + kGroupRows);
+        u.clear();
+        for (int r = r0; r < r1; r++) {
+            if (X.doff[r + 1] - X.doff[r] != nd) return JCI_ERR_SPACE;
+            for (long long k = X.doff[r]; k < X.doff[r + 1]; k++) u.push_back(X.doub[k].target);
+        }
+        std::sort(u.begin(), u.end());
+        u.erase(std::unique(u.begin(), u.end()), u.end());
+        if (u.size() > 65535) return JCI_ERR_SPACE;
+        for (int r = r0; r < r1; r++)
+            for (int f = 0; f < nd; f++) {
+                const int tgt = X.doub[X.doff[r] + f].target;
+                upos[(size_t)f * n + r] =
+                    (uint16_t)(std::lower_bound(u.begin(), u.end(), tgt) - u.begin());
+            }
+        const size_t padded = (u.size() + 3) / 4 * 4;
+        while (u.size() < padded) u.push_back(u[0]);
+        uidx.insert(uidx.end(), u.begin(), u.end());
+        uoff[g + 1] = (int)uidx.size();
+    }
+    GroupTables h;
+    h.ng = ng;
+    h.rows = n;
+    h.nd = nd;
+    h.nu = uidx.size();
+    jci_status r = JCI_OK;
+    if (cudaMalloc(&h.uoff, uoff.size() * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&h.uidx, uidx.size() * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&h.upos, upos.size() * sizeof(uint16_t)) != cudaSuccess ||
+        cudaMalloc(&h.c64, h.nu * kGroupRows * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&h.c32, h.nu * kGroupRows * sizeof(float)) != cudaSuccess)
+        r = JCI_ERR_CUDA;
+    if (!r && (cudaMemcpy(h.uoff, uoff.data(), uoff.size() * sizeof(int),
+                          cudaMemcpyHostToDevice) != cudaSuccess ||
+               cudaMemcpy(h.uidx, uidx.data(), uidx.size() * sizeof(int),
+                          cudaMemcpyHostToDevice) != cudaSuccess ||
+               cudaMemcpy(h.upos, upos.data(), upos.size() * sizeof(uint16_t),
+                          cudaMemcpyHostToDevice) != cudaSuccess))
+        r = JCI_ERR_CUDA;
+    if (r) {
+        group_tables_free(&h);
+        return r;
+    }
+    *t = h;
+    return JCI_OK;
+}
+
+void group_tables_free(GroupTables *t) {
+    cudaFree(t->uoff);
+    cudaFree(t->uidx);
+    cudaFree(t->upos);
+    cudaFree(t->c64);
+    cudaFree(t->c32);
+    *t = GroupTables();
+}
+
+// Coefficient blocks from the current double values ([double][string], FP64
+// and FP32), on stream st.
+jci_status group_fill(GroupTables *t, const double *dblH, const float *dblHf, cudaStream_t st) {
+    JCI_CUDA(cudaMemsetAsync(t->c64, 0, t->nu * kGroupRows * sizeof(double), st));
+    JCI_CUDA(cudaMemsetAsync(t->c32, 0, t->nu * kGroupRows * sizeof(float), st));
+    const long long n = (long long)t->rows * t->nd;
+    const int grid = (int)std::min<long long>((n + 255) / 256, 4096);
+    k_group_coef<double><<<grid, 256, 0, st>>>(t->rows, t->nd, dblH, t->upos, t->uoff, t->c64);
+    k_group_coef<float><<<grid, 256, 0, st>>>(t->rows, t->nd, dblHf, t->upos, t->uoff, t->c32);
+    JCI_CUDA(cudaGetLastError());
+    return JCI_OK;
+}
+
+// Columns per thread: two only in FP32 (in FP64 the 32 accumulators would
+// halve the resident CTAs).
+int group_items(int len, size_t w) { return w == sizeof(float) && len > 256 ? 2 : 1; }
+
+// 256-thread CTAs (256 ITEMS columns each), or 128-thread ones when the
+// wider CTAs would give fewer than four per SM (small spaces).
+template <typename T>
+jci_status group_launch(const GroupArgs<T> &a, int items, int device, const T *x, T *y,
+                        cudaStream_t st) {
+    if (items != 1 && items != 2) return JCI_ERR_ARG;
+    int nsm = 0;
+    JCI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    const int ng = (a.rows + kGroupRows - 1) / kGroupRows;
+    const long long wide = (long long)ng * ((a.len + 256 * items - 1) / (256 * items));
+    const int nt = wide < 4LL * nsm ? 128 : 256;
+    const int seg = nt * items;
+    const dim3 grid(ng, (a.len + seg - 1) / seg);
+#define JCI_GROUP(NT, IT) \
+    if (nt == NT && items == IT) k_sigma_group<T, NT, IT><<<grid, NT, 0, st>>>(a, x, y);
+    JCI_GROUP(128, 1)
+    JCI_GROUP(128, 2)
+    JCI_GROUP(256, 1)
+    JCI_GROUP(256, 2)
+#undef JCI_GROUP
+    JCI_CUDA(cudaGetLastError());
+    return JCI_OK;
+}
+
+template jci_status group_launch<double>(const GroupArgs<double> &, int, int, const double *,
+                                         double *, cudaStream_t);
+template jci_status group_launch<float>(const GroupArgs<float> &, int, int, const float *, float *,
+                                        cudaStream_t);
+
+}  // namespace jci

@@ -52,6 +52,34 @@ template <typename T>
 jci_status ab_launch(const AbArgs<T> &a, int tx, int device, const T *v, T *o,
                      cudaStream_t st);
 
+// Same-spin doubles over groups of consecutive strings, jci_fci_group.cu.
+constexpr int kGroupRows = 16;
+template <typename T>
+struct GroupArgs {
+    int rows, len;          // output rows (strings of the spin) x row length
+    const int *uoff;        // [group + 1] first union entry of each group
+    const int *uidx;        // union entries: source rows
+    const T *coef;          // [entry][kGroupRows] double values (0: not reached)
+    const T *hd;            // [row][column] diagonal, or null
+    int add;                // 1: Y += result, 0: Y = result
+    const int *skip;        // nonzero: return at once
+};
+struct GroupTables {
+    int ng = 0, rows = 0, nd = 0;
+    size_t nu = 0;          // union entries over all groups
+    int *uoff = nullptr, *uidx = nullptr;
+    uint16_t *upos = nullptr;   // [double][string] position in the group's union
+    double *c64 = nullptr;
+    float *c32 = nullptr;
+};
+jci_status group_tables_build(const jci_space *s, int spin, GroupTables *t);
+void group_tables_free(GroupTables *t);
+jci_status group_fill(GroupTables *t, const double *dblH, const float *dblHf, cudaStream_t st);
+int group_items(int len, size_t w);
+template <typename T>
+jci_status group_launch(const GroupArgs<T> &a, int items, int device, const T *x, T *y,
+                        cudaStream_t st);
+
 // Generic path (any truncated space), jci_device.cu.
 jci_status device_sigma_generic(jci_space *s, int nvec, const void *vin, void *sout,
                                 long long ld, int precision, cudaStream_t st);
