@@ -75,8 +75,8 @@ def sigma_plan_desc(mode, nt, R, B):
           else "row_kernel_threads"): nt,
          ("staged_rows" if mode == 0 else
           "product_column_threads" if mode in (4, 5, 7) else "product_ctas_per_sm"): R}
-    if not groups:
-        d["beta_pass_threads" if streams else "rows_per_cta"] = B
+    d["beta_pass_threads" if streams else "group_columns_per_thread" if groups
+      else "rows_per_cta"] = B
     return d
 
 

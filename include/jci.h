@@ -198,7 +198,8 @@ jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sigma,
  * SM, 0 = as many as fit; modes 4, 5, 7: column threads of the fused
  * product, 8 or 16), `batch` (modes 1, 2, 5: alpha strings per CTA of the
  * row kernel; modes 3-4: threads per CTA of the beta pass; modes 6-7:
- * unused), and its timed cost in ms per vector.  All 0 before the first sigma call and on the
+ * columns per thread of the group kernel, 1 or 2), and its timed cost in
+ * ms per vector.  All 0 before the first sigma call and on the
  * multi-group path.  No reference counterpart (the reference has no device
  * tuning). */
 jci_status jci_sigma_tuning(const jci_space *s, int precision, int *mode,

@@ -1136,10 +1136,10 @@ static jci_status group_tables(jci_space *s, cudaStream_t st) {
 static bool group_possible(const FciTables *f) { return f->da >= 1 && f->db >= 1; }
 
 // Doubles of spin sp by groups: rows x len matrix x -> y (add: y += ...),
-// with the diagonal hd when given.
+// with the diagonal hd when given; items = columns per thread (1 or 2).
 template <typename T>
 static jci_status launch_group(jci_space *s, int sp, const T *hd, int add, const int *skip,
-                               const T *x, T *y, cudaStream_t st) {
+                               int items, const T *x, T *y, cudaStream_t st) {
     FciTables *f = s->dev->fci;
     jci_status r = group_tables(s, st);
     if (r) return r;
@@ -1156,7 +1156,7 @@ static jci_status launch_group(jci_space *s, int sp, const T *hd, int add, const
     g.hd = hd;
     g.add = add;
     g.skip = skip;
-    return group_launch<T>(g, group_items(g.len, sizeof(T)), s->dev->device, x, y, st);
+    return group_launch<T>(g, items, s->dev->device, x, y, st);
 }
 
 // Scratch of the streaming plan: C^T and the beta part, N each, allocated on
@@ -1204,9 +1204,9 @@ static jci_status launch_transposes(const FciTables *f, const T *v, T *ct, T *o,
 // modes 3, 4: row streams on C^T (B threads) and C (nt threads), then the
 //   product: 3: k_sigma_mixed (R CTAs per SM), 4: k_sigma_ab (R column
 //   threads).
-// modes 6, 7: the same-spin doubles by string groups on C and C^T, the beta
-//   singles as a row stream on C^T (nt threads), then the product of mode 3
-//   (6) or of mode 4 (7).
+// modes 6, 7: the same-spin doubles by string groups on C and C^T (B
+//   columns per thread), the beta singles as a row stream on C^T (nt
+//   threads), then the product of mode 3 (6) or of mode 4 (7).
 template <typename T>
 static jci_status run_plan(jci_space *s, FciArgs<T> a, int mode, int nt, int R, int B,
                            const T *v, T *o, cudaStream_t st) {
@@ -1221,8 +1221,8 @@ static jci_status run_plan(jci_space *s, FciArgs<T> a, int mode, int nt, int R, 
         be.nd = 0;  // the beta doubles come from the group kernel
         if ((r = launch_transposes<T>(f, v, ct, o, tau, false, a.skip, st))) return r;
         if ((r = launch_stream<T>(be, nt, ct, tau, st))) return r;
-        if ((r = launch_group<T>(s, 1, nullptr, 1, a.skip, ct, tau, st))) return r;
-        if ((r = launch_group<T>(s, 0, a.hd, 0, a.skip, v, o, st))) return r;
+        if ((r = launch_group<T>(s, 1, nullptr, 1, a.skip, B, ct, tau, st))) return r;
+        if ((r = launch_group<T>(s, 0, a.hd, 0, a.skip, B, v, o, st))) return r;
         if ((r = launch_transposes<T>(f, v, ct, o, tau, true, a.skip, st))) return r;
         a.do_as = 0;
         a.R = 0;
@@ -1380,7 +1380,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     }
     // modes 6, 7: the doubles by string groups, the beta singles as a stream
     float best6 = 1e30f;
-    int b6s = 0;
+    int b6s = 0, b6i = 1;
     if (bsprod < 1e30f && group_possible(f) && !err) {
         T *ct = nullptr, *tau = nullptr;
         err = stream_scratch<T>(f, &ct, &tau);
@@ -1393,10 +1393,14 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
             float ms = timeit([&] { return launch_stream<T>(be, nt, ct, tau, st); });
             if (ms < bs) { bs = ms; b6s = nt; }
         }
-        float gg = timeit([&] {
-            jci_status q = launch_group<T>(s, 1, nullptr, 1, nullptr, ct, tau, st);
-            return q ? q : launch_group<T>(s, 0, a.hd, 0, nullptr, v, o, st);
-        });
+        float gg = 1e30f;
+        for (int it : {1, 2}) {
+            float ms = timeit([&] {
+                jci_status q = launch_group<T>(s, 1, nullptr, 1, nullptr, it, ct, tau, st);
+                return q ? q : launch_group<T>(s, 0, a.hd, 0, nullptr, it, v, o, st);
+            });
+            if (ms < gg) { gg = ms; b6i = it; }
+        }
         float tt = timeit([&] {
             jci_status q = launch_transposes<T>(f, v, ct, o, tau, false, nullptr, st);
             return q ? q : launch_transposes<T>(f, v, ct, o, tau, true, nullptr, st);
@@ -1418,7 +1422,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     if (b3a && b3b)
         best3 = best_of([&] { return run_plan<T>(s, a, smode, b3a, sR, b3b, v, o, st); });
     if (best6 < 1e30f)
-        best6 = best_of([&] { return run_plan<T>(s, a, gmode, b6s, sR, 1, v, o, st); });
+        best6 = best_of([&] { return run_plan<T>(s, a, gmode, b6s, sR, b6i, v, o, st); });
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(v);
@@ -1434,7 +1438,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     f->tuned_mode[prec] = mode;
     f->tuned_nt[prec] = groups ? b6s : streams ? b3a : mode ? b1nt : b0nt;
     f->tuned_R[prec] = (streams || groups) ? sR : mode ? b1R : b0R;
-    f->tuned_B[prec] = groups ? 1 : streams ? b3b : mode ? b1B : 1;
+    f->tuned_B[prec] = groups ? b6i : streams ? b3b : mode ? b1B : 1;
     f->tuned_ms[prec] = best;
     // drop the group tables unless a precision uses them
     const int other = f->tuned_mode[prec ^ 1];
@@ -1523,7 +1527,7 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, 
     size_t w = p ? sizeof(float) : sizeof(double);
     if (mode == 6 || mode == 7) {
         bool ok = mode == 6 ? mixed_possible(f, w) && R >= 0 : ab_plan_possible(f, R, w);
-        if (!ok || !group_possible(f) || !stream_ok(f->na, nt) ||
+        if (!ok || !group_possible(f) || !stream_ok(f->na, nt) || (B != 1 && B != 2) ||
             stream_smem(0, f->sb, w) > f->smem_max)
             return JCI_ERR_ARG;
     } else if (mode == 3 || mode == 4) {

@@ -26,6 +26,17 @@ namespace jci {
 namespace {
 
 constexpr int kGroupChunk = 64;  // source rows per staged coefficient chunk
+
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<double> {
+    using type = double2;
+};
+template <>
+struct Vec16<float> {
+    using type = float4;
+};
 constexpr int kGroupAhead = 8;   // source rows loaded ahead per thread
 
 // Y[I][c] for the kGroupRows rows of group blockIdx.x and the columns
@@ -76,12 +87,19 @@ __global__ void __launch_bounds__(NT)
         }
 #pragma unroll
         for (int q = 0; q < Q; q++) {
-            const T *h = cs[b][k + q];
+            // the row's coefficients as 16-byte broadcast loads
+            using V = typename Vec16<T>::type;
+            constexpr int E = 16 / (int)sizeof(T);
+            const V *h = reinterpret_cast<const V *>(cs[b][k + q]);
 #pragma unroll
-            for (int r = 0; r < RG; r++) {
-                const T hr = h[r];
+            for (int p = 0; p < RG / E; p++) {
+                const V hv = h[p];
+                const T *he = reinterpret_cast<const T *>(&hv);
 #pragma unroll
-                for (int i = 0; i < ITEMS; i++) acc[r][i] = fma(hr, x[q][i], acc[r][i]);
+                for (int e = 0; e < E; e++)
+#pragma unroll
+                    for (int i = 0; i < ITEMS; i++)
+                        acc[p * E + e][i] = fma(he[e], x[q][i], acc[p * E + e][i]);
             }
         }
     };
@@ -210,10 +228,6 @@ jci_status group_fill(GroupTables *t, const double *dblH, const float *dblHf, cu
     JCI_CUDA(cudaGetLastError());
     return JCI_OK;
 }
-
-// Columns per thread: two only in FP32 (in FP64 the 32 accumulators would
-// halve the resident CTAs).
-int group_items(int len, size_t w) { return w == sizeof(float) && len > 256 ? 2 : 1; }
 
 // 256-thread CTAs (256 ITEMS columns each), or 128-thread ones when the
 // wider CTAs would give fewer than four per SM (small spaces).

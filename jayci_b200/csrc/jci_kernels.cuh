@@ -75,7 +75,6 @@ struct GroupTables {
 jci_status group_tables_build(const jci_space *s, int spin, GroupTables *t);
 void group_tables_free(GroupTables *t);
 jci_status group_fill(GroupTables *t, const double *dblH, const float *dblHf, cudaStream_t st);
-int group_items(int len, size_t w);
 template <typename T>
 jci_status group_launch(const GroupArgs<T> &a, int items, int device, const T *x, T *y,
                         cudaStream_t st);
