@@ -15,12 +15,9 @@
 // taken in one fixed order (chunk, then list) and results are bitwise
 // reproducible; T never leaves the SM.
 //
-// Three product engines:
-//  - k_sigma_ab_ws (FP64, 32-column chunks): the FP64 tensor cores,
-//    mma.sync m8n8k4 (tcgen05 has no FP64 kind), warp-specialised: four
-//    warps multiply chunk c+1 while four gather chunk c;
-//  - k_sigma_ab_dmma (FP64, 64-column chunks): the same tensor-core tiles,
-//    every warp multiplying and then gathering, with the chunk's entry
+// Two product engines:
+//  - k_sigma_ab_dmma (FP64, 64-column chunks): the FP64 tensor cores,
+//    mma.sync m8n8k4 (tcgen05 has no FP64 kind), with the chunk's entry
 //    lists copied into shared memory (cp.async) while the chunk multiplies;
 //  - k_sigma_ab (FP32 and FP64, 32- or 64-column chunks): register tiles on
 //    the CUDA-core FMA pipes, entry lists read from L2.
@@ -319,182 +316,6 @@ __global__ void __launch_bounds__(kAbThreads, 1)
     }
 }
 
-// ---- FP64 tensor-core engine, warp-specialised ------------------------------
-//
-// 32-column chunks.  Warps 0-3 multiply: warp (wm, wn) = (w / 2, w % 2)
-// owns the 8x8 tiles of rows 8 (wm MTW + i) (i < MTW) and columns 16 wn +
-// 8 j (j < 2), and writes its tiles of chunk c into T buffer c % 2.  Warps
-// 4-7 gather chunk c (strings Ib = t + 128 i) from that buffer while chunk
-// c+1 multiplies.  Hand-off through named barriers: FULL[b] (the product
-// warps arrive after writing buffer b, the gather warps wait) and EMPTY[b]
-// (the gather warps arrive after reading it, the product warps wait before
-// rewriting it); every arrival is matched by one wait within the same alpha
-// string, so the barriers are balanced when the next string starts.
-constexpr int kWsCW = 32, kWsCWP = 36;  // chunk columns; B row stride (4 mod 16)
-constexpr int kBarFull = 1, kBarEmpty = 3, kBarMma = 5, kBarGather = 6;
-
-__device__ __forceinline__ void named_sync(int id, int n) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
-}
-__device__ __forceinline__ void named_arrive(int id, int n) {
-    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
-}
-
-template <int MTW, int ITEMS>
-__global__ void __launch_bounds__(kAbThreads, 1)
-    k_sigma_ab_ws(AbArgs<double> a, const double *__restrict__ V, double *__restrict__ S) {
-    if (a.skip && *a.skip) return;
-    constexpr int R8 = 16 * MTW;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int K = a.sa, K4 = dm_k4(K), KP = dm_kp(K), nb = a.nb, mrows = a.mrows;
-    double *As = reinterpret_cast<double *>(smem_raw);             // [R8][KP]
-    double *Bs = As + (size_t)R8 * KP;                             // [2][K4][kWsCWP]
-    double *Ts = Bs + 2 * (size_t)K4 * kWsCWP;                     // [2][mrows][kWsCW]
-    uint32_t *es = reinterpret_cast<uint32_t *>(Ts + 2 * (size_t)mrows * kWsCW);  // [2][maxent]
-    uint16_t *os = reinterpret_cast<uint16_t *>(es + 2 * (size_t)a.maxent);      // [2][offs]
-    int *jl = reinterpret_cast<int *>(os + 2 * (size_t)a.offs);                  // [K]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const bool mma = warp < 4;
-    const int gt = tid & 127;  // thread index within its group
-    for (int idx = tid; idx < 2 * (K4 - K) * kWsCWP; idx += kAbThreads) {
-        const int b = idx / ((K4 - K) * kWsCWP), r = idx % ((K4 - K) * kWsCWP);
-        Bs[(size_t)b * K4 * kWsCWP + (size_t)K * kWsCWP + r] = 0.0;
-    }
-    for (int Ia = blockIdx.x; Ia < a.na; Ia += gridDim.x) {
-        __syncthreads();
-        for (int idx = tid; idx < R8 * K4; idx += kAbThreads) {
-            const int m = idx / K4, j = idx - m * K4;
-            double v = 0.0;
-            if (j < K && m <= a.npair) {
-                const long long o = (long long)j * a.na + Ia;
-                v = m < a.npair ? a.m2[eri_index(a.fpA[o], m)] : a.a1A[o];
-                if (a.fsA[o] >> 31) v = -v;
-            }
-            As[(size_t)m * KP + j] = v;
-        }
-        for (int j = tid; j < K; j += kAbThreads)
-            jl[j] = (int)(a.fsA[(long long)j * a.na + Ia] & 0x3fffffffu);
-        __syncthreads();
-        if (mma) {
-            const int g = lane >> 2, t = lane & 3, wn = warp & 1, wm = warp >> 1;
-            auto stage_b = [&](int c, double *buf) {
-                const int c0 = c * kWsCW;
-                if (a.vec) {
-                    for (int idx = gt; idx < K * (kWsCW / 2); idx += 128) {
-                        const int j = idx / (kWsCW / 2), cc = 2 * (idx % (kWsCW / 2)),
-                                  col = c0 + cc;
-                        double *dst = buf + (size_t)j * kWsCWP + cc;
-                        if (col < nb)
-                            __pipeline_memcpy_async(dst, V + (long long)jl[j] * nb + col, 16);
-                        else
-                            dst[0] = dst[1] = 0.0;
-                    }
-                } else {
-                    for (int idx = gt; idx < K * kWsCW; idx += 128) {
-                        const int j = idx / kWsCW, cc = idx % kWsCW, col = c0 + cc;
-                        double *dst = buf + (size_t)j * kWsCWP + cc;
-                        if (col < nb)
-                            __pipeline_memcpy_async(dst, V + (long long)jl[j] * nb + col, 8);
-                        else
-                            dst[0] = 0.0;
-                    }
-                }
-                __pipeline_commit();
-            };
-            stage_b(0, Bs);
-            for (int ci = 0; ci < a.nchunk; ci++) {
-                const int buf = ci & 1;
-                __pipeline_wait_prior(0);
-                named_sync(kBarMma, 128);  // B chunk ci landed; chunk ci-1 fully read
-                if (ci + 1 < a.nchunk) stage_b(ci + 1, Bs + (size_t)(buf ^ 1) * K4 * kWsCWP);
-                const double *Bc = Bs + (size_t)buf * K4 * kWsCWP;
-                double acc[MTW][2][2];
-#pragma unroll
-                for (int i = 0; i < MTW; i++)
-#pragma unroll
-                    for (int j = 0; j < 2; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
-                const double *ap = As + (size_t)(8 * wm * MTW + g) * KP + t;
-                const double *bp = Bc + (size_t)t * kWsCWP + 16 * wn + g;
-#pragma unroll 2
-                for (int k0 = 0; k0 < K4; k0 += 4) {
-                    const double b0 = bp[(size_t)k0 * kWsCWP], b1 = bp[(size_t)k0 * kWsCWP + 8];
-#pragma unroll
-                    for (int i = 0; i < MTW; i++) {
-                        const double av = ap[(size_t)8 * i * KP + k0];
-                        ab_dmma(acc[i][0], av, b0);
-                        ab_dmma(acc[i][1], av, b1);
-                    }
-                }
-                if (ci >= 2) named_sync(kBarEmpty + buf, kAbThreads);  // gather of ci-2 done
-                double *Tb = Ts + (size_t)buf * mrows * kWsCW;
-#pragma unroll
-                for (int i = 0; i < MTW; i++) {
-                    const int m = 8 * (wm * MTW + i) + g;
-                    if (m < mrows) {
-#pragma unroll
-                        for (int j = 0; j < 2; j++) {
-                            double *dst = Tb + (size_t)m * kWsCW + 16 * wn + 8 * j + 2 * t;
-                            dst[0] = acc[i][j][0];
-                            dst[1] = acc[i][j][1];
-                        }
-                    }
-                }
-                named_arrive(kBarFull + buf, kAbThreads);
-            }
-            // the gather's arrivals for the last two chunks
-            for (int ci = max(0, a.nchunk - 2); ci < a.nchunk; ci++)
-                named_sync(kBarEmpty + (ci & 1), kAbThreads);
-        } else {
-            auto stage_l = [&](int c, int buf) {
-                const uint16_t *og = a.off + (size_t)c * a.offs;
-                uint16_t *od = os + (size_t)buf * a.offs;
-                for (int idx = gt; idx < a.offs / 8; idx += 128)
-                    __pipeline_memcpy_async(od + 8 * idx, og + 8 * idx, 16);
-                const uint32_t b0 = a.base[c], n4 = (a.base[c + 1] - b0) / 4;
-                uint32_t *ed = es + (size_t)buf * a.maxent;
-                for (uint32_t idx = gt; idx < n4; idx += 128)
-                    __pipeline_memcpy_async(ed + 4 * idx, a.ent + b0 + 4 * idx, 16);
-                __pipeline_commit();
-            };
-            double x[ITEMS];
-#pragma unroll
-            for (int i = 0; i < ITEMS; i++) x[i] = 0.0;
-            stage_l(0, 0);
-            for (int ci = 0; ci < a.nchunk; ci++) {
-                const int buf = ci & 1;
-                __pipeline_wait_prior(0);
-                named_sync(kBarGather, 128);  // lists of ci landed; chunk ci-1 fully read
-                if (ci + 1 < a.nchunk) stage_l(ci + 1, buf ^ 1);
-                named_sync(kBarFull + buf, kAbThreads);  // T chunk ci written
-                const double *Tb = Ts + (size_t)buf * mrows * kWsCW;
-                const uint16_t *ob = os + (size_t)buf * a.offs;
-                const uint32_t *eb = es + (size_t)buf * a.maxent;
-#pragma unroll
-                for (int i = 0; i < ITEMS; i++) {
-                    const int Ib = gt + 128 * i;
-                    if (Ib < nb) {
-                        const int k1 = ob[Ib + 1];
-                        double sacc = x[i];
-                        for (int k = ob[Ib]; k < k1; k++) {
-                            const uint32_t e = eb[k];
-                            const double v = Tb[(size_t)((e >> 8) & 0xffffu) * kWsCW + (e & 0xffu)];
-                            sacc += e >> 31 ? -v : v;
-                        }
-                        x[i] = sacc;
-                    }
-                }
-                named_arrive(kBarEmpty + buf, kAbThreads);
-            }
-            double *srow = S + (long long)Ia * nb;
-#pragma unroll
-            for (int i = 0; i < ITEMS; i++) {
-                const int Ib = gt + 128 * i;
-                if (Ib < nb) srow[Ib] += x[i];
-            }
-        }
-    }
-}
-
 template <typename T>
 using AbKernel = void (*)(AbArgs<T>, const T *, T *);
 
@@ -536,31 +357,9 @@ AbKernel<double> dmma_kernel_mt(int mtw) {
     }
 }
 
-template <int ITEMS>
-AbKernel<double> ws_kernel_mt(int mtw) {
-    switch (mtw) {
-        case 1: return k_sigma_ab_ws<1, ITEMS>;
-        case 2: return k_sigma_ab_ws<2, ITEMS>;
-        case 3: return k_sigma_ab_ws<3, ITEMS>;
-        case 4: return k_sigma_ab_ws<4, ITEMS>;
-        case 5: return k_sigma_ab_ws<5, ITEMS>;
-        case 6: return k_sigma_ab_ws<6, ITEMS>;
-        case 7: return k_sigma_ab_ws<7, ITEMS>;
-        case 8: return k_sigma_ab_ws<8, ITEMS>;
-        case 9: return k_sigma_ab_ws<9, ITEMS>;
-        default: return nullptr;
-    }
-}
-
 int ab_items(int nb) {
     const int it = (nb + kAbThreads - 1) / kAbThreads;
     return it <= 4 ? 4 : it <= 16 ? 16 : 0;
-}
-
-// strings per gather thread of the warp-specialised engine (128 threads)
-int ws_items(int nb) {
-    const int it = (nb + 127) / 128;
-    return it <= 8 ? 8 : it <= 16 ? 16 : it <= 32 ? 32 : 0;
 }
 
 int ab_tm(int mrows, int tx) { return (mrows + kAbThreads / tx - 1) / (kAbThreads / tx); }
@@ -568,26 +367,14 @@ int ab_tm(int mrows, int tx) { return (mrows + kAbThreads / tx - 1) / (kAbThread
 // m tiles per warp of the tensor-core engine (two warp rows of 8-row tiles)
 int dm_mtw(int mrows) { return ((mrows + 7) / 8 + 1) / 2; }
 
-// In FP64 the tensor cores run both chunk widths: 64 columns with every
-// warp multiplying and then gathering (tx = 16), 32 columns warp-
-// specialised (tx = 8).
+// The tensor-core engine runs FP64 chunks of 64 columns (tx = 16).
 bool use_dmma(int tx, size_t w) { return tx == 16 && w == sizeof(double); }
-bool use_ws(int tx, size_t w) { return tx == 8 && w == sizeof(double); }
 
 template <typename T>
 AbKernel<T> ab_kernel(int tx, int mrows, int items) {
     if constexpr (sizeof(T) == sizeof(double)) {
         if (use_dmma(tx, sizeof(T)))
             return items == 4 ? dmma_kernel_mt<4>(dm_mtw(mrows)) : dmma_kernel_mt<16>(dm_mtw(mrows));
-        if (use_ws(tx, sizeof(T))) {
-            const int mtw = dm_mtw(mrows);
-            switch (items) {
-                case 8: return ws_kernel_mt<8>(mtw);
-                case 16: return ws_kernel_mt<16>(mtw);
-                case 32: return ws_kernel_mt<32>(mtw);
-                default: return nullptr;
-            }
-        }
     }
     const int tm = ab_tm(mrows, tx);
     if (tx == 8) return items == 4 ? ab_kernel_tm<T, 8, 4>(tm) : ab_kernel_tm<T, 8, 16>(tm);
@@ -604,30 +391,24 @@ int ab_maxent(const AbShape &sh, int cw) { return (cw * (1 + sh.nelb + sh.sb) + 
 
 }  // namespace
 
-// Dynamic shared memory of each engine; maxent, offs: longest chunk list
-// and offset row stride of the tx tables.
-static size_t ab_smem_bytes(int tx, size_t w, int sa, int mrows, int maxent, int offs) {
-    if (use_dmma(tx, w) || use_ws(tx, w)) {
-        const int K4 = dm_k4(sa), KP = dm_kp(sa), R8 = 16 * dm_mtw(mrows);
-        const bool ws = use_ws(tx, w);
-        const int cw = ws ? kWsCW : kDmCW, cwp = ws ? kWsCWP : kDmCWP, nbuf = ws ? 2 : 1;
-        return ((size_t)R8 * KP + 2 * (size_t)K4 * cwp + (size_t)nbuf * mrows * cw) * w +
-               (size_t)nbuf * ((size_t)maxent * 4 + (size_t)offs * 2) + (size_t)sa * 4 + 16;
+size_t ab_smem(const AbShape &sh, int tx, size_t w) {
+    const int mrows = sh.npair + 1;
+    if (use_dmma(tx, w)) {
+        const int K4 = dm_k4(sh.sa), KP = dm_kp(sh.sa), R8 = 16 * dm_mtw(mrows);
+        return ((size_t)R8 * KP + 2 * (size_t)K4 * kDmCWP + (size_t)mrows * kDmCW) * w +
+               (size_t)ab_maxent(sh, kDmCW) * 4 + (size_t)ab_offs(sh.nb) * 2 +
+               (size_t)sh.sa * 4 + 16;
     }
     const int cw = 4 * tx, mp = (kAbThreads / tx) * ab_tm(mrows, tx);
-    return ((size_t)sa * mp + 2 * (size_t)sa * cw + (size_t)mrows * cw) * w + (size_t)sa * 4 + 16;
-}
-
-size_t ab_smem(const AbShape &sh, int tx, size_t w) {
-    return ab_smem_bytes(tx, w, sh.sa, sh.npair + 1, ab_maxent(sh, 4 * tx), ab_offs(sh.nb));
+    return ((size_t)sh.sa * mp + 2 * (size_t)sh.sa * cw + (size_t)mrows * cw) * w +
+           (size_t)sh.sa * 4 + 16;
 }
 
 bool ab_possible(const AbShape &sh, int tx, size_t w, size_t smem_max) {
     const int mrows = sh.npair + 1;
     if (tx != 8 && tx != 16) return false;
     if (!ab_items(sh.nb) || sh.sa < 1 || mrows > 65535) return false;
-    if (use_ws(tx, w) && !ws_items(sh.nb)) return false;
-    if (use_dmma(tx, w) || use_ws(tx, w)) {
+    if (use_dmma(tx, w)) {
         if (dm_mtw(mrows) > 9) return false;
     } else if (ab_tm(mrows, tx) > (tx == 16 ? 9 : 5)) {
         return false;
@@ -722,10 +503,19 @@ void ab_tables_free(AbTables *t) {
 template <typename T>
 jci_status ab_launch(const AbArgs<T> &a, int tx, int device, const T *v, T *o,
                      cudaStream_t st) {
-    const int items = use_ws(tx, sizeof(T)) ? ws_items(a.nb) : ab_items(a.nb);
+    const int items = ab_items(a.nb);
     AbKernel<T> kern = items ? ab_kernel<T>(tx, a.mrows, items) : nullptr;
     if (!kern || a.nchunk != (a.nb + 4 * tx - 1) / (4 * tx)) return JCI_ERR_SPACE;
-    const size_t smem = ab_smem_bytes(tx, sizeof(T), a.sa, a.mrows, a.maxent, a.offs);
+    size_t smem;
+    if (use_dmma(tx, sizeof(T))) {
+        const int K4 = dm_k4(a.sa), KP = dm_kp(a.sa), R8 = 16 * dm_mtw(a.mrows);
+        smem = ((size_t)R8 * KP + 2 * (size_t)K4 * kDmCWP + (size_t)a.mrows * kDmCW) * sizeof(T) +
+               (size_t)a.maxent * 4 + (size_t)a.offs * 2 + (size_t)a.sa * 4 + 16;
+    } else {
+        const int cw = 4 * tx, mp = (kAbThreads / tx) * ab_tm(a.mrows, tx);
+        smem = ((size_t)a.sa * mp + 2 * (size_t)a.sa * cw + (size_t)a.mrows * cw) * sizeof(T) +
+               (size_t)a.sa * 4 + 16;
+    }
     JCI_CUDA(smem_optin(kern));
     int occ = 0, nsm = 0;
     JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kAbThreads, smem));
