@@ -1149,6 +1149,7 @@ static jci_status launch_group(jci_space *s, int sp, const T *hd, int add, const
     g.len = sp == 0 ? f->nb : f->na;
     g.uoff = t.uoff;
     g.uidx = t.uidx;
+    g.useg = t.useg;
     if constexpr (sizeof(T) == sizeof(double))
         g.coef = t.c64;
     else

@@ -8,14 +8,15 @@
 // with H[I][J] the double's value with phase, or 0 when I does not reach J.
 // Consecutive strings share most targets (16 rows of FCI(14,14) reach 3.7x
 // fewer distinct rows than they have doubles), so every source row
-// segment is read from L2 once per group instead of once per row; the
-// zeros of the kGroupRows x |U_G| coefficient block cost FMAs, not bytes.
-// The sums run in a fixed order (U_G ascending), so results are bitwise
+// segment is read from L2 once per group instead of once per row.  The
+// union is sorted by the set of row quads (rows 4q..4q+3) that reach each
+// entry, and each such class runs a loop compiled for its quads, so the
+// zero coefficients of the other quads cost neither bytes nor FMAs.  The
+// sums run in a fixed order (class, then string), so results are bitwise
 // reproducible.
 #include <cuda_pipeline.h>
 
 #include <algorithm>
-#include <type_traits>
 #include <vector>
 
 #include "jci_internal.h"
@@ -24,8 +25,6 @@
 namespace jci {
 
 namespace {
-
-constexpr int kGroupChunk = 64;  // source rows per staged coefficient chunk
 
 template <typename T>
 struct Vec16;
@@ -37,28 +36,81 @@ template <>
 struct Vec16<float> {
     using type = float4;
 };
-constexpr int kGroupAhead = 8;   // source rows loaded ahead per thread
+
+constexpr int kGroupChunk = 64;  // union entries per staged chunk
+
+// The entries k0..k1-1 of the staged chunk (coefficient rows cs, source
+// rows js) that belong to class QM: reached only by the row quads set in
+// QM (bit q: rows 4q..4q+3), so the FMAs of the other quads, whose
+// coefficients are all zero, are not issued.  k1 - k0 is a multiple of 4.
+template <typename T, int ITEMS, int QM>
+__device__ __forceinline__ void group_class(T (&acc)[kGroupRows][ITEMS],
+                                            const T *__restrict__ X,
+                                            const T (*__restrict__ cs)[kGroupRows],
+                                            const int *__restrict__ js, const int (&col)[ITEMS],
+                                            const bool (&in)[ITEMS], int len, int k0, int k1) {
+    using V = typename Vec16<T>::type;
+    constexpr int E = 16 / (int)sizeof(T);  // rows per 16-byte piece
+    constexpr int QE = 4 / E;               // pieces per row quad
+    for (int k = k0; k < k1; k += 4) {
+        T x[4][ITEMS];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const T *src = X + (long long)js[k + q] * len;
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) x[q][i] = in[i] ? src[col[i]] : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const V *h = reinterpret_cast<const V *>(cs[k + q]);
+#pragma unroll
+            for (int qd = 0; qd < 4; qd++) {
+                if ((QM >> qd) & 1) {  // a constant once the loop is unrolled
+#pragma unroll
+                    for (int pe = 0; pe < QE; pe++) {
+                        const V hv = h[qd * QE + pe];
+                        const T *he = reinterpret_cast<const T *>(&hv);
+#pragma unroll
+                        for (int e = 0; e < E; e++) {
+                            const int r = 4 * qd + pe * E + e;
+#pragma unroll
+                            for (int i = 0; i < ITEMS; i++)
+                                acc[r][i] = fma(he[e], x[q][i], acc[r][i]);
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
 
 // Y[I][c] for the kGroupRows rows of group blockIdx.x and the columns
-// c0 + tid + NT i (i < ITEMS) of segment blockIdx.y.
+// c0 + tid + NT i (i < ITEMS) of segment blockIdx.y.  The group's union
+// entries come sorted by class (the set of row quads that reach them), and
+// class QM covers entries useg[g][QM] .. useg[g][QM + 1] - 1; chunks of
+// kGroupChunk entries are staged in shared memory (cp.async, double-
+// buffered) and each class's part of a chunk runs its own loop.
 template <typename T, int NT, int ITEMS>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 512 / NT)  // at least 16 warps per SM
     k_sigma_group(GroupArgs<T> a, const T *__restrict__ X, T *__restrict__ Y) {
     if (a.skip && *a.skip) return;
     constexpr int RG = kGroupRows;
     __shared__ __align__(16) T cs[2][kGroupChunk][RG];
     __shared__ int js[2][kGroupChunk];
+    __shared__ int sg[17];
     const int g = blockIdx.x, tid = threadIdx.x, len = a.len;
     const int r0 = g * RG, nr = min(RG, a.rows - r0);
     const int c0 = blockIdx.y * (NT * ITEMS);
-    const long long u0 = a.uoff[g], u1 = a.uoff[g + 1];
-    auto stage = [&](long long u, int b) {
-        const int n = (int)min((long long)kGroupChunk, u1 - u);
+    const int u0 = a.uoff[g], u1 = a.uoff[g + 1];
+    if (tid < 17) sg[tid] = a.useg[(size_t)g * 17 + tid];
+    auto stage = [&](int u, int b) {
+        const int n = min(kGroupChunk, u1 - u);
         // coefficient rows are RG * sizeof(T) bytes: 16-byte pieces
         constexpr int per = RG * (int)sizeof(T) / 16;
         for (int idx = tid; idx < n * per; idx += NT)
             __pipeline_memcpy_async(reinterpret_cast<char *>(&cs[b][0][0]) + 16 * idx,
-                                    reinterpret_cast<const char *>(a.coef + u * RG) + 16 * idx,
+                                    reinterpret_cast<const char *>(a.coef + (size_t)u * RG) +
+                                        16 * idx,
                                     16);
         for (int idx = tid; idx < n; idx += NT) js[b][idx] = a.uidx[u + idx];
         __pipeline_commit();
@@ -75,45 +127,35 @@ __global__ void __launch_bounds__(NT)
         col[i] = c0 + tid + NT * i;
         in[i] = col[i] < len;
     }
-    // one step: Q source rows loaded, then their FMAs
-    auto step = [&](int b, int k, auto qn) {
-        constexpr int Q = decltype(qn)::value;
-        T x[Q][ITEMS];
-#pragma unroll
-        for (int q = 0; q < Q; q++) {
-            const T *src = X + (long long)js[b][k + q] * len;
-#pragma unroll
-            for (int i = 0; i < ITEMS; i++) x[q][i] = in[i] ? src[col[i]] : T(0);
-        }
-#pragma unroll
-        for (int q = 0; q < Q; q++) {
-            // the row's coefficients as 16-byte broadcast loads
-            using V = typename Vec16<T>::type;
-            constexpr int E = 16 / (int)sizeof(T);
-            const V *h = reinterpret_cast<const V *>(cs[b][k + q]);
-#pragma unroll
-            for (int p = 0; p < RG / E; p++) {
-                const V hv = h[p];
-                const T *he = reinterpret_cast<const T *>(&hv);
-#pragma unroll
-                for (int e = 0; e < E; e++)
-#pragma unroll
-                    for (int i = 0; i < ITEMS; i++)
-                        acc[p * E + e][i] = fma(he[e], x[q][i], acc[p * E + e][i]);
-            }
-        }
-    };
     if (u0 < u1) stage(u0, 0);
     int b = 0;
-    for (long long u = u0; u < u1; u += kGroupChunk, b ^= 1) {
+    for (int u = u0; u < u1; u += kGroupChunk, b ^= 1) {
         __pipeline_wait_prior(0);
         __syncthreads();  // chunk b landed; every thread is done with chunk b^1
         if (u + kGroupChunk < u1) stage(u + kGroupChunk, b ^ 1);
-        const int n = (int)min((long long)kGroupChunk, u1 - u);  // a multiple of 4
-        int k = 0;
-        for (; k + kGroupAhead <= n; k += kGroupAhead)
-            step(b, k, std::integral_constant<int, kGroupAhead>());
-        for (; k < n; k += 4) step(b, k, std::integral_constant<int, 4>());
+        const int ue = min(u + kGroupChunk, u1);
+#define JCI_CLASS(QM)                                                                   \
+    {                                                                                   \
+        const int lo = max(sg[QM], u), hi = min(sg[QM + 1], ue);                        \
+        if (lo < hi)                                                                    \
+            group_class<T, ITEMS, QM>(acc, X, cs[b], js[b], col, in, len, lo - u, hi - u); \
+    }
+        JCI_CLASS(1)
+        JCI_CLASS(2)
+        JCI_CLASS(3)
+        JCI_CLASS(4)
+        JCI_CLASS(5)
+        JCI_CLASS(6)
+        JCI_CLASS(7)
+        JCI_CLASS(8)
+        JCI_CLASS(9)
+        JCI_CLASS(10)
+        JCI_CLASS(11)
+        JCI_CLASS(12)
+        JCI_CLASS(13)
+        JCI_CLASS(14)
+        JCI_CLASS(15)
+#undef JCI_CLASS
     }
 #pragma unroll
     for (int r = 0; r < RG; r++) {
@@ -148,17 +190,19 @@ __global__ void k_group_coef(int nstr, int nd, const T *__restrict__ dblH,
 }  // namespace
 
 // Host structure of the groups of one spin (integral-independent): the
-// sorted union of each group's double targets, padded with zero-coefficient
-// copies of its first entry to a multiple of 4, and every double's position
-// in its group's union.  The coefficients are filled on the device
-// (group_fill) from the current double values.
+// union of each group's double targets, sorted by class (the set of row
+// quads that reach an entry, 1..15) and within a class by string, every
+// class padded with zero-coefficient copies of its first entry to a
+// multiple of 4; the class boundaries; every double's position in its
+// group's union.  The coefficients are filled on the device (group_fill)
+// from the current double values.
 jci_status group_tables_build(const jci_space *s, int spin, GroupTables *t) {
     const SpinSpace &X = s->sp[spin];
     const int n = X.nstr, nd = X.max_doub, ng = (n + kGroupRows - 1) / kGroupRows;
     if (n < 1 || nd < 1) return JCI_ERR_SPACE;
-    std::vector<int> uoff(ng + 1, 0), uidx;
+    std::vector<int> uoff(ng + 1, 0), uidx, useg((size_t)ng * 17);
     std::vector<uint16_t> upos((size_t)nd * n);
-    std::vector<int> u;
+    std::vector<int> u, list;
     for (int g = 0; g < ng; g++) {
         const int r0 = g * kGroupRows, r1 = std::min(n, r0 + kGroupRows);
         u.clear();
@@ -168,26 +212,48 @@ jci_status group_tables_build(const jci_space *s, int spin, GroupTables *t) {
         }
         std::sort(u.begin(), u.end());
         u.erase(std::unique(u.begin(), u.end()), u.end());
-        if (u.size() > 65535) return JCI_ERR_SPACE;
+        // row quads reaching each entry
+        std::vector<int> qm(u.size(), 0);
+        for (int r = r0; r < r1; r++)
+            for (int f = 0; f < nd; f++) {
+                const int tgt = X.doub[X.doff[r] + f].target;
+                qm[std::lower_bound(u.begin(), u.end(), tgt) - u.begin()] |= 1 << ((r - r0) / 4);
+            }
+        list.clear();
+        std::vector<int> where(u.size());
+        useg[(size_t)g * 17] = (int)uidx.size();
+        for (int c = 1; c <= 15; c++) {
+            useg[(size_t)g * 17 + c] = (int)(uidx.size() + list.size());
+            const size_t first = list.size();
+            for (size_t e = 0; e < u.size(); e++)
+                if (qm[e] == c) {
+                    where[e] = (int)(uidx.size() + list.size()) - uoff[g];
+                    list.push_back(u[e]);
+                }
+            if (list.size() > first)
+                while ((list.size() - first) % 4) list.push_back(list[first]);
+        }
+        useg[(size_t)g * 17 + 16] = (int)(uidx.size() + list.size());
+        if (list.size() > 65535) return JCI_ERR_SPACE;
         for (int r = r0; r < r1; r++)
             for (int f = 0; f < nd; f++) {
                 const int tgt = X.doub[X.doff[r] + f].target;
                 upos[(size_t)f * n + r] =
-                    (uint16_t)(std::lower_bound(u.begin(), u.end(), tgt) - u.begin());
+                    (uint16_t)where[std::lower_bound(u.begin(), u.end(), tgt) - u.begin()];
             }
-        const size_t padded = (u.size() + 3) / 4 * 4;
-        while (u.size() < padded) u.push_back(u[0]);
-        uidx.insert(uidx.end(), u.begin(), u.end());
+        uidx.insert(uidx.end(), list.begin(), list.end());
         uoff[g + 1] = (int)uidx.size();
     }
     GroupTables h;
     h.ng = ng;
     h.rows = n;
     h.nd = nd;
-    h.nu = uidx.size();
+    h.nu = std::max<size_t>(uidx.size(), 1);
+    uidx.resize(h.nu, 0);
     jci_status r = JCI_OK;
     if (cudaMalloc(&h.uoff, uoff.size() * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&h.uidx, uidx.size() * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&h.useg, useg.size() * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&h.upos, upos.size() * sizeof(uint16_t)) != cudaSuccess ||
         cudaMalloc(&h.c64, h.nu * kGroupRows * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&h.c32, h.nu * kGroupRows * sizeof(float)) != cudaSuccess)
@@ -195,6 +261,8 @@ jci_status group_tables_build(const jci_space *s, int spin, GroupTables *t) {
     if (!r && (cudaMemcpy(h.uoff, uoff.data(), uoff.size() * sizeof(int),
                           cudaMemcpyHostToDevice) != cudaSuccess ||
                cudaMemcpy(h.uidx, uidx.data(), uidx.size() * sizeof(int),
+                          cudaMemcpyHostToDevice) != cudaSuccess ||
+               cudaMemcpy(h.useg, useg.data(), useg.size() * sizeof(int),
                           cudaMemcpyHostToDevice) != cudaSuccess ||
                cudaMemcpy(h.upos, upos.data(), upos.size() * sizeof(uint16_t),
                           cudaMemcpyHostToDevice) != cudaSuccess))
@@ -210,6 +278,7 @@ jci_status group_tables_build(const jci_space *s, int spin, GroupTables *t) {
 void group_tables_free(GroupTables *t) {
     cudaFree(t->uoff);
     cudaFree(t->uidx);
+    cudaFree(t->useg);
     cudaFree(t->upos);
     cudaFree(t->c64);
     cudaFree(t->c32);

@@ -59,6 +59,7 @@ struct GroupArgs {
     int rows, len;          // output rows (strings of the spin) x row length
     const int *uoff;        // [group + 1] first union entry of each group
     const int *uidx;        // union entries: source rows
+    const int *useg;        // [group][17] class boundaries (class q: row quads q)
     const T *coef;          // [entry][kGroupRows] double values (0: not reached)
     const T *hd;            // [row][column] diagonal, or null
     int add;                // 1: Y += result, 0: Y = result
@@ -68,6 +69,7 @@ struct GroupTables {
     int ng = 0, rows = 0, nd = 0;
     size_t nu = 0;          // union entries over all groups
     int *uoff = nullptr, *uidx = nullptr;
+    int *useg = nullptr;        // [group][17] class boundaries of the union
     uint16_t *upos = nullptr;   // [double][string] position in the group's union
     double *c64 = nullptr;
     float *c32 = nullptr;
