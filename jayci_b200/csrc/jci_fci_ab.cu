@@ -175,23 +175,23 @@ __host__ __device__ inline int dm_kp(int K) {
     return k4 + (20 - k4 % 16) % 16;
 }
 
-template <int MTW, int ITEMS>
-__global__ void __launch_bounds__(kAbThreads, 1)
+template <int MTW, int ITEMS, int NB>
+__global__ void __launch_bounds__(kAbThreads, NB == 1 ? 2 : 1)  // one B buffer: two CTAs per SM
     k_sigma_ab_dmma(AbArgs<double> a, const double *__restrict__ V, double *__restrict__ S) {
     if (a.skip && *a.skip) return;
     constexpr int R8 = 16 * MTW;  // product rows covered (>= mrows)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = a.sa, K4 = dm_k4(K), KP = dm_kp(K), nb = a.nb;
     double *As = reinterpret_cast<double *>(smem_raw);             // [R8][KP]
-    double *Bs = As + (size_t)R8 * KP;                             // [2][K4][kDmCWP]
-    double *Ts = Bs + 2 * (size_t)K4 * kDmCWP;                     // [mrows][kDmCW]
+    double *Bs = As + (size_t)R8 * KP;                             // [NB][K4][kDmCWP]
+    double *Ts = Bs + NB * (size_t)K4 * kDmCWP;                    // [mrows][kDmCW]
     uint32_t *es = reinterpret_cast<uint32_t *>(Ts + (size_t)a.mrows * kDmCW);  // [maxent]
     uint16_t *os = reinterpret_cast<uint16_t *>(es + a.maxent);   // [offs]
     int *jl = reinterpret_cast<int *>(os + a.offs);                // [K]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3, wn = warp & 3, wm = warp >> 2;
-    // the k rows K..K4-1 of both B buffers stay zero (never staged)
-    for (int idx = tid; idx < 2 * (K4 - K) * kDmCWP; idx += kAbThreads) {
+    // the k rows K..K4-1 of the B buffers stay zero (never staged)
+    for (int idx = tid; idx < NB * (K4 - K) * kDmCWP; idx += kAbThreads) {
         const int b = idx / ((K4 - K) * kDmCWP), r = idx % ((K4 - K) * kDmCWP);
         Bs[(size_t)b * K4 * kDmCWP + (size_t)K * kDmCWP + r] = 0.0;
     }
@@ -249,14 +249,15 @@ __global__ void __launch_bounds__(kAbThreads, 1)
         __syncthreads();
         stage_b(0, Bs);
         for (int ci = 0; ci < a.nchunk; ci++) {
-            const double *Bc = Bs + (size_t)(ci & 1) * K4 * kDmCWP;
+            const double *Bc = Bs + (size_t)(ci % NB) * K4 * kDmCWP;
             // B chunk ci landed; every thread is past the previous gather, so
-            // the lists and the other B buffer may be overwritten
+            // the lists (and, double-buffered, the other B buffer) may be
+            // overwritten
             __pipeline_wait_prior(0);
             __syncthreads();
             stage_l(ci);
             const bool more = ci + 1 < a.nchunk;
-            if (more) stage_b(ci + 1, Bs + (size_t)((ci + 1) & 1) * K4 * kDmCWP);
+            if (NB == 2 && more) stage_b(ci + 1, Bs + (size_t)((ci + 1) & 1) * K4 * kDmCWP);
             double acc[MTW][2][2];
 #pragma unroll
             for (int i = 0; i < MTW; i++)
@@ -287,11 +288,13 @@ __global__ void __launch_bounds__(kAbThreads, 1)
                     }
                 }
             }
-            if (more)
+            if (NB == 2 && more)
                 __pipeline_wait_prior(1);  // the lists (B chunk ci+1 may still fly)
             else
                 __pipeline_wait_prior(0);
             __syncthreads();
+            // single-buffered: chunk ci+1 is copied while chunk ci gathers
+            if (NB == 1 && more) stage_b(ci + 1, Bs);
 #pragma unroll
             for (int i = 0; i < ITEMS; i++) {
                 const int Ib = tid + kAbThreads * i;
@@ -341,18 +344,18 @@ AbKernel<T> ab_kernel_tm(int tm) {
     return nullptr;
 }
 
-template <int ITEMS>
+template <int ITEMS, int NB>
 AbKernel<double> dmma_kernel_mt(int mtw) {
     switch (mtw) {
-        case 1: return k_sigma_ab_dmma<1, ITEMS>;
-        case 2: return k_sigma_ab_dmma<2, ITEMS>;
-        case 3: return k_sigma_ab_dmma<3, ITEMS>;
-        case 4: return k_sigma_ab_dmma<4, ITEMS>;
-        case 5: return k_sigma_ab_dmma<5, ITEMS>;
-        case 6: return k_sigma_ab_dmma<6, ITEMS>;
-        case 7: return k_sigma_ab_dmma<7, ITEMS>;
-        case 8: return k_sigma_ab_dmma<8, ITEMS>;
-        case 9: return k_sigma_ab_dmma<9, ITEMS>;
+        case 1: return k_sigma_ab_dmma<1, ITEMS, NB>;
+        case 2: return k_sigma_ab_dmma<2, ITEMS, NB>;
+        case 3: return k_sigma_ab_dmma<3, ITEMS, NB>;
+        case 4: return k_sigma_ab_dmma<4, ITEMS, NB>;
+        case 5: return k_sigma_ab_dmma<5, ITEMS, NB>;
+        case 6: return k_sigma_ab_dmma<6, ITEMS, NB>;
+        case 7: return k_sigma_ab_dmma<7, ITEMS, NB>;
+        case 8: return k_sigma_ab_dmma<8, ITEMS, NB>;
+        case 9: return k_sigma_ab_dmma<9, ITEMS, NB>;
         default: return nullptr;
     }
 }
@@ -371,10 +374,14 @@ int dm_mtw(int mrows) { return ((mrows + 7) / 8 + 1) / 2; }
 bool use_dmma(int tx, size_t w) { return tx == 16 && w == sizeof(double); }
 
 template <typename T>
-AbKernel<T> ab_kernel(int tx, int mrows, int items) {
+AbKernel<T> ab_kernel(int tx, int mrows, int items, int nbuf) {
     if constexpr (sizeof(T) == sizeof(double)) {
-        if (use_dmma(tx, sizeof(T)))
-            return items == 4 ? dmma_kernel_mt<4>(dm_mtw(mrows)) : dmma_kernel_mt<16>(dm_mtw(mrows));
+        if (use_dmma(tx, sizeof(T))) {
+            const int mtw = dm_mtw(mrows);
+            if (nbuf == 1)
+                return items == 4 ? dmma_kernel_mt<4, 1>(mtw) : dmma_kernel_mt<16, 1>(mtw);
+            return items == 4 ? dmma_kernel_mt<4, 2>(mtw) : dmma_kernel_mt<16, 2>(mtw);
+        }
     }
     const int tm = ab_tm(mrows, tx);
     if (tx == 8) return items == 4 ? ab_kernel_tm<T, 8, 4>(tm) : ab_kernel_tm<T, 8, 16>(tm);
@@ -391,17 +398,20 @@ int ab_maxent(const AbShape &sh, int cw) { return (cw * (1 + sh.nelb + sh.sb) + 
 
 }  // namespace
 
-size_t ab_smem(const AbShape &sh, int tx, size_t w) {
-    const int mrows = sh.npair + 1;
+// Dynamic shared memory of each engine; nbuf: B buffers of the tensor-core
+// engine; maxent, offs: longest chunk list and offset row stride.
+static size_t ab_smem_bytes(int tx, size_t w, int sa, int mrows, int nbuf, int maxent, int offs) {
     if (use_dmma(tx, w)) {
-        const int K4 = dm_k4(sh.sa), KP = dm_kp(sh.sa), R8 = 16 * dm_mtw(mrows);
-        return ((size_t)R8 * KP + 2 * (size_t)K4 * kDmCWP + (size_t)mrows * kDmCW) * w +
-               (size_t)ab_maxent(sh, kDmCW) * 4 + (size_t)ab_offs(sh.nb) * 2 +
-               (size_t)sh.sa * 4 + 16;
+        const int K4 = dm_k4(sa), KP = dm_kp(sa), R8 = 16 * dm_mtw(mrows);
+        return ((size_t)R8 * KP + (size_t)nbuf * K4 * kDmCWP + (size_t)mrows * kDmCW) * w +
+               (size_t)maxent * 4 + (size_t)offs * 2 + (size_t)sa * 4 + 16;
     }
     const int cw = 4 * tx, mp = (kAbThreads / tx) * ab_tm(mrows, tx);
-    return ((size_t)sh.sa * mp + 2 * (size_t)sh.sa * cw + (size_t)mrows * cw) * w +
-           (size_t)sh.sa * 4 + 16;
+    return ((size_t)sa * mp + 2 * (size_t)sa * cw + (size_t)mrows * cw) * w + (size_t)sa * 4 + 16;
+}
+
+size_t ab_smem(const AbShape &sh, int tx, size_t w) {
+    return ab_smem_bytes(tx, w, sh.sa, sh.npair + 1, 2, ab_maxent(sh, 4 * tx), ab_offs(sh.nb));
 }
 
 bool ab_possible(const AbShape &sh, int tx, size_t w, size_t smem_max) {
@@ -504,21 +514,21 @@ template <typename T>
 jci_status ab_launch(const AbArgs<T> &a, int tx, int device, const T *v, T *o,
                      cudaStream_t st) {
     const int items = ab_items(a.nb);
-    AbKernel<T> kern = items ? ab_kernel<T>(tx, a.mrows, items) : nullptr;
-    if (!kern || a.nchunk != (a.nb + 4 * tx - 1) / (4 * tx)) return JCI_ERR_SPACE;
-    size_t smem;
-    if (use_dmma(tx, sizeof(T))) {
-        const int K4 = dm_k4(a.sa), KP = dm_kp(a.sa), R8 = 16 * dm_mtw(a.mrows);
-        smem = ((size_t)R8 * KP + 2 * (size_t)K4 * kDmCWP + (size_t)a.mrows * kDmCW) * sizeof(T) +
-               (size_t)a.maxent * 4 + (size_t)a.offs * 2 + (size_t)a.sa * 4 + 16;
-    } else {
-        const int cw = 4 * tx, mp = (kAbThreads / tx) * ab_tm(a.mrows, tx);
-        smem = ((size_t)a.sa * mp + 2 * (size_t)a.sa * cw + (size_t)a.mrows * cw) * sizeof(T) +
-               (size_t)a.sa * 4 + 16;
-    }
-    JCI_CUDA(smem_optin(kern));
+    if (!items || a.nchunk != (a.nb + 4 * tx - 1) / (4 * tx)) return JCI_ERR_SPACE;
+    // The tensor-core engine single-buffers its B chunks when that lets two
+    // CTAs share an SM (the other CTA hides the copy); else it double-buffers.
+    AbKernel<T> kern = nullptr;
+    size_t smem = 0;
     int occ = 0, nsm = 0;
-    JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kAbThreads, smem));
+    for (int nbuf : {1, 2}) {
+        if (nbuf == 1 && !use_dmma(tx, sizeof(T))) continue;
+        kern = ab_kernel<T>(tx, a.mrows, items, nbuf);
+        if (!kern) return JCI_ERR_SPACE;
+        smem = ab_smem_bytes(tx, sizeof(T), a.sa, a.mrows, nbuf, a.maxent, a.offs);
+        JCI_CUDA(smem_optin(kern));
+        JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kAbThreads, smem));
+        if (nbuf == 2 || occ >= 2) break;
+    }
     if (occ < 1) return JCI_ERR_SPACE;
     JCI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     const int grid = std::max(1, std::min(a.na, nsm * occ));
