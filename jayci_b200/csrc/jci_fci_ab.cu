@@ -48,17 +48,37 @@ __device__ __forceinline__ void ab_dmma(double (&d)[2], double a, double b) {
 
 // ---- CUDA-core engine -------------------------------------------------------
 //
-// TX threads across the chunk's columns (4 columns each, interleaved by TX,
-// so CW = 4 TX), TY = 256 / TX threads across the product rows (TM rows
-// each); ITEMS beta strings per thread in the gather.
+// TX threads across the chunk's columns (4 consecutive columns each, so
+// CW = 4 TX), TY = 256 / TX threads across the product rows (TM rows each);
+// ITEMS beta strings per thread in the gather.  A thread's TM rows of A
+// are stored padded to TMP (a multiple of 16 bytes), so per k step it
+// reads its A values and its four B values with 16-byte loads.
+template <typename T>
+struct AbVec;
+template <>
+struct AbVec<double> {
+    using type = double2;
+};
+template <>
+struct AbVec<float> {
+    using type = float4;
+};
+
+__host__ __device__ constexpr int ab_tmp(int tm, int w) {
+    return (tm + 16 / w - 1) / (16 / w) * (16 / w);
+}
+
 template <typename T, int TX, int TM, int ITEMS>
 __global__ void __launch_bounds__(kAbThreads)
     k_sigma_ab(AbArgs<T> a, const T *__restrict__ V, T *__restrict__ S) {
     if (a.skip && *a.skip) return;
-    constexpr int TY = kAbThreads / TX, CW = 4 * TX, MP = TY * TM;
+    using VT = typename AbVec<T>::type;
+    constexpr int E = 16 / (int)sizeof(T);  // values per 16-byte load
+    constexpr int TMP = ab_tmp(TM, (int)sizeof(T));
+    constexpr int TY = kAbThreads / TX, CW = 4 * TX, MP = TY * TMP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = a.sa, nb = a.nb;
-    T *As = reinterpret_cast<T *>(smem_raw);                        // [K][MP]
+    T *As = reinterpret_cast<T *>(smem_raw);                        // [K][TY][TMP]
     T *Bs = As + (size_t)K * MP;                                    // [2][K][CW]
     T *Ts = Bs + 2 * (size_t)K * CW;                                // [mrows][CW]
     int *jl = reinterpret_cast<int *>(Ts + (size_t)a.mrows * CW);  // [K]
@@ -79,14 +99,15 @@ __global__ void __launch_bounds__(kAbThreads)
     for (int Ia = blockIdx.x; Ia < a.na; Ia += gridDim.x) {
         __syncthreads();
         for (int idx = tid; idx < K * MP; idx += kAbThreads) {
-            const int j = idx / MP, m = idx - j * MP;
+            const int j = idx / MP, pos = idx - j * MP, i = pos % TMP;
+            const int m = i < TM ? (pos / TMP) * TM + i : a.mrows;  // padding: zero
             const long long o = (long long)j * a.na + Ia;
             const uint32_t e = a.fsA[o];
             T v = T(0);
             if (m < a.npair) v = a.m2[eri_index(a.fpA[o], m)];
             else if (m == a.npair) v = a.a1A[o];
             As[idx] = ab_flip(v, e >> 31);
-            if (m == 0) jl[j] = (int)(e & 0x3fffffffu);
+            if (pos == 0) jl[j] = (int)(e & 0x3fffffffu);
         }
         T x[ITEMS];
 #pragma unroll
@@ -110,26 +131,26 @@ __global__ void __launch_bounds__(kAbThreads)
                 for (int q = 0; q < 4; q++) acc[i][q] = T(0);
 #pragma unroll 4
             for (int k = 0; k < K; k++) {
-                // columns tx + TX q: a warp reads TX consecutive words per load
-                const T *br = Bc + k * CW + tx;
-                const T b0 = br[0], b1 = br[TX], b2 = br[2 * TX], b3 = br[3 * TX];
-                const T *ar = As + k * MP + ty * TM;
+                // columns 4 tx .. 4 tx + 3 and the thread's A rows, 16 bytes a load
+                T bv[4], av[TMP];
+                const VT *br = reinterpret_cast<const VT *>(Bc + k * CW + 4 * tx);
 #pragma unroll
-                for (int i = 0; i < TM; i++) {
-                    const T av = ar[i];
-                    acc[i][0] = fma(av, b0, acc[i][0]);
-                    acc[i][1] = fma(av, b1, acc[i][1]);
-                    acc[i][2] = fma(av, b2, acc[i][2]);
-                    acc[i][3] = fma(av, b3, acc[i][3]);
-                }
+                for (int q = 0; q < 4 / E; q++) *reinterpret_cast<VT *>(bv + q * E) = br[q];
+                const VT *ar = reinterpret_cast<const VT *>(As + k * MP + ty * TMP);
+#pragma unroll
+                for (int q = 0; q < TMP / E; q++) *reinterpret_cast<VT *>(av + q * E) = ar[q];
+#pragma unroll
+                for (int i = 0; i < TM; i++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) acc[i][q] = fma(av[i], bv[q], acc[i][q]);
             }
 #pragma unroll
             for (int i = 0; i < TM; i++) {
                 const int m = ty * TM + i;
                 if (m < a.mrows) {
-                    T *dst = Ts + (size_t)m * CW + tx;
+                    T *dst = Ts + (size_t)m * CW + 4 * tx;
 #pragma unroll
-                    for (int q = 0; q < 4; q++) dst[q * TX] = acc[i][q];
+                    for (int q = 0; q < 4; q++) dst[q] = acc[i][q];
                 }
             }
             __syncthreads();
@@ -406,7 +427,7 @@ static size_t ab_smem_bytes(int tx, size_t w, int sa, int mrows, int nbuf, int m
         return ((size_t)R8 * KP + (size_t)nbuf * K4 * kDmCWP + (size_t)mrows * kDmCW) * w +
                (size_t)maxent * 4 + (size_t)offs * 2 + (size_t)sa * 4 + 16;
     }
-    const int cw = 4 * tx, mp = (kAbThreads / tx) * ab_tm(mrows, tx);
+    const int cw = 4 * tx, mp = (kAbThreads / tx) * ab_tmp(ab_tm(mrows, tx), (int)w);
     return ((size_t)sa * mp + 2 * (size_t)sa * cw + (size_t)mrows * cw) * w + (size_t)sa * 4 + 16;
 }
 
