@@ -292,35 +292,14 @@ struct MixArgs {
     const int *skip;
 };
 
-// A thread's TM rows of A are stored padded to a multiple of 16 bytes (TMP)
-// and its four columns are consecutive, so each k step reads them with
-// 16-byte loads.
-template <typename T>
-struct MixVec;
-template <>
-struct MixVec<double> {
-    using type = double2;
-};
-template <>
-struct MixVec<float> {
-    using type = float4;
-};
-
-__host__ __device__ constexpr int mix_tmp(int tm, int w) {
-    return (tm + 16 / w - 1) / (16 / w) * (16 / w);
-}
-
 template <typename T, int TM>
 __global__ void __launch_bounds__(kMixThreads)
     k_sigma_mixed(MixArgs<T> a, const T *__restrict__ V, T *__restrict__ S, T *__restrict__ Tbuf) {
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using VT = typename MixVec<T>::type;
-    constexpr int E = 16 / (int)sizeof(T);
-    constexpr int TMP = mix_tmp(TM, (int)sizeof(T));
-    constexpr int MP = 16 * TMP;
+    constexpr int MP = 16 * TM;
     const int K = a.sa;
-    T *As = reinterpret_cast<T *>(smem_raw);          // [K][16][TMP]
+    T *As = reinterpret_cast<T *>(smem_raw);          // [K][MP]
     T *Bs = As + (size_t)K * MP;                      // [2][K][64]
     int *jl = reinterpret_cast<int *>(Bs + 2 * (size_t)K * kMixCols);  // [K]
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
@@ -342,15 +321,14 @@ __global__ void __launch_bounds__(kMixThreads)
     for (int Ia = blockIdx.x; Ia < a.na; Ia += gridDim.x) {
         __syncthreads();
         for (int idx = tid; idx < K * MP; idx += kMixThreads) {
-            const int j = idx / MP, pos = idx - j * MP, i = pos % TMP;
-            const int m = i < TM ? (pos / TMP) * TM + i : a.mrows;  // padding: zero
+            int j = idx / MP, m = idx - j * MP;
             long long o = (long long)j * a.na + Ia;
             uint32_t e = a.fsA[o];
             T v = T(0);
             if (m < a.npair) v = a.m2[eri_index(a.fpA[o], m)];
             else if (m == a.npair) v = a.a1A[o];
             As[idx] = flip(v, e >> 31);
-            if (pos == 0) jl[j] = (int)(e & 0x3fffffffu);
+            if (m == 0) jl[j] = (int)(e & 0x3fffffffu);
         }
         __syncthreads();
         stage(0, Bs);
@@ -371,27 +349,27 @@ __global__ void __launch_bounds__(kMixThreads)
                 for (int q = 0; q < 4; q++) acc[i][q] = T(0);
 #pragma unroll 4
             for (int k = 0; k < K; k++) {
-                // thread tx owns columns 4tx..4tx+3; A rows and B columns
-                // arrive with 16-byte loads
-                T bv[4], av[TMP];
-                const VT *br = reinterpret_cast<const VT *>(Bc + k * kMixCols + 4 * tx);
+                // thread tx owns columns tx, tx+16, tx+32, tx+48: a warp
+                // reads 16 consecutive words per load (no bank conflicts)
+                const T *br = Bc + k * kMixCols + tx;
+                T b0 = br[0], b1 = br[16], b2 = br[32], b3 = br[48];
+                const T *ar = As + k * MP + ty * TM;
 #pragma unroll
-                for (int q = 0; q < 4 / E; q++) *reinterpret_cast<VT *>(bv + q * E) = br[q];
-                const VT *ar = reinterpret_cast<const VT *>(As + k * MP + ty * TMP);
-#pragma unroll
-                for (int q = 0; q < TMP / E; q++) *reinterpret_cast<VT *>(av + q * E) = ar[q];
-#pragma unroll
-                for (int i = 0; i < TM; i++)
-#pragma unroll
-                    for (int q = 0; q < 4; q++) acc[i][q] = fma(av[i], bv[q], acc[i][q]);
+                for (int i = 0; i < TM; i++) {
+                    T av = ar[i];
+                    acc[i][0] = fma(av, b0, acc[i][0]);
+                    acc[i][1] = fma(av, b1, acc[i][1]);
+                    acc[i][2] = fma(av, b2, acc[i][2]);
+                    acc[i][3] = fma(av, b3, acc[i][3]);
+                }
             }
 #pragma unroll
             for (int i = 0; i < TM; i++) {
                 int m = ty * TM + i;
                 if (m < a.mrows) {
-                    T *dst = Tb + (size_t)m * a.nbp + c0 + 4 * tx;
+                    T *dst = Tb + (size_t)m * a.nbp + c0 + tx;
 #pragma unroll
-                    for (int q = 0; q < 4; q++) dst[q] = acc[i][q];
+                    for (int q = 0; q < 4; q++) dst[16 * q] = acc[i][q];
                 }
             }
             __syncthreads();
@@ -840,8 +818,7 @@ static size_t rows_smem(int nb, int npair, int da, int RB, size_t w) {
 }
 
 static size_t mix_smem(int K, int TM, size_t w) {
-    return (size_t)K * 16 * mix_tmp(TM, (int)w) * w + 2 * (size_t)K * kMixCols * w +
-           (size_t)K * 4 + 16;
+    return (size_t)K * 16 * TM * w + 2 * (size_t)K * kMixCols * w + (size_t)K * 4 + 16;
 }
 
 static size_t fci_smem(int nb, int npair, int R, size_t w) {
