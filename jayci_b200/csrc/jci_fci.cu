@@ -1106,7 +1106,7 @@ static jci_status launch_ab(jci_space *s, const FciArgs<T> &fa, const T *v, T *o
     m.nchunk = t->nchunk;
     m.offs = t->offs;
     m.maxent = t->maxent;
-    m.vec = (fa.nb % 2 == 0 && reinterpret_cast<uintptr_t>(v) % 16 == 0) ? 1 : 0;
+    m.vec = ((size_t)fa.nb * sizeof(T) % 16 == 0 && reinterpret_cast<uintptr_t>(v) % 16 == 0) ? 1 : 0;
     m.fsA = fa.fsA; m.fpA = fa.fpA; m.a1A = fa.a1A; m.m2 = fa.m2;
     m.off = t->off; m.base = t->base; m.ent = t->ent;
     m.skip = fa.skip;

@@ -15,12 +15,15 @@
 // taken in one fixed order (chunk, then list) and results are bitwise
 // reproducible; T never leaves the SM.
 //
-// Two product engines:
+// Three product engines:
 //  - k_sigma_ab_dmma (FP64, 64-column chunks): the FP64 tensor cores,
 //    mma.sync m8n8k4 (tcgen05 has no FP64 kind), with the chunk's entry
 //    lists copied into shared memory (cp.async) while the chunk multiplies;
-//  - k_sigma_ab (FP32 and FP64, 32- or 64-column chunks): register tiles on
-//    the CUDA-core FMA pipes, entry lists read from L2.
+//  - k_sigma_ab_tf32 (FP32, 64-column chunks): the same structure on the
+//    TF32 tensor cores with 3xTF32 operand splitting (FP32 accuracy, FP32
+//    accumulation);
+//  - k_sigma_ab (FP32 and FP64, 32-column chunks): register tiles on the
+//    CUDA-core FMA pipes, entry lists read from L2.
 #include <cuda_pipeline.h>
 
 #include <algorithm>
@@ -340,6 +343,203 @@ __global__ void __launch_bounds__(kAbThreads, NB == 1 ? 2 : 1)  // one B buffer:
     }
 }
 
+// ---- FP32 tensor-core engine: 3xTF32 -----------------------------------------
+//
+// The FP32 product on the tensor cores with FP32 accuracy: each FP32
+// operand x is split into a TF32 part x_h = tf32(x) and a TF32 remainder
+// x_l = tf32(x - x_h), and every 16x8x8 tile takes three mma.sync.m16n8k8
+// with FP32 accumulation, a_l b_h + a_h b_l + a_h b_h (the a_l b_l term is
+// below FP32 rounding).  64-column chunks; eight warps as 2 (rows) x 4
+// (columns): warp (wm, wn) owns the 16x8 tiles of rows 16 (wm MT + i) (i <
+// MT) and columns 16 wn + 8 j (j < 2).  Row strides are padded (4 mod 32
+// words for A, 8 mod 32 for B) so the fragment loads hit distinct banks.
+// Chunk lists, gather and buffering as in k_sigma_ab_dmma.
+constexpr int kTfCW = 64, kTfCWP = 72;
+
+__host__ __device__ inline int tf_k8(int K) { return (K + 7) & ~7; }
+__host__ __device__ inline int tf_kp(int K) {
+    const int k8 = tf_k8(K);
+    return k8 + (36 - k8 % 32) % 32;
+}
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ void split_tf32(float x, uint32_t &hi, uint32_t &lo) {
+    hi = to_tf32(x);
+    lo = to_tf32(x - __uint_as_float(hi));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <int MT, int ITEMS, int NB>
+__global__ void __launch_bounds__(kAbThreads, NB == 1 ? 2 : 1)  // one B buffer: two CTAs per SM
+    k_sigma_ab_tf32(AbArgs<float> a, const float *__restrict__ V, float *__restrict__ S) {
+    if (a.skip && *a.skip) return;
+    constexpr int R16 = 32 * MT;  // product rows covered (>= mrows)
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int K = a.sa, K8 = tf_k8(K), KP = tf_kp(K), nb = a.nb;
+    float *As = reinterpret_cast<float *>(smem_raw);               // [R16][KP]
+    float *Bs = As + (size_t)R16 * KP;                             // [NB][K8][kTfCWP]
+    float *Ts = Bs + NB * (size_t)K8 * kTfCWP;                     // [mrows][kTfCW]
+    uint32_t *es = reinterpret_cast<uint32_t *>(Ts + (size_t)a.mrows * kTfCW);  // [maxent]
+    uint16_t *os = reinterpret_cast<uint16_t *>(es + a.maxent);   // [offs]
+    int *jl = reinterpret_cast<int *>(os + a.offs);                // [K]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3, wn = warp & 3, wm = warp >> 2;
+    // the k rows K..K8-1 of the B buffers stay zero (never staged)
+    for (int idx = tid; idx < NB * (K8 - K) * kTfCWP; idx += kAbThreads) {
+        const int b = idx / ((K8 - K) * kTfCWP), r = idx % ((K8 - K) * kTfCWP);
+        Bs[(size_t)b * K8 * kTfCWP + (size_t)K * kTfCWP + r] = 0.f;
+    }
+    auto stage_b = [&](int c, float *buf) {
+        const int c0 = c * kTfCW;
+        if (a.vec) {  // nb a multiple of 4 and C 16-byte aligned: column quads
+            for (int idx = tid; idx < K * (kTfCW / 4); idx += kAbThreads) {
+                const int j = idx / (kTfCW / 4), cc = 4 * (idx % (kTfCW / 4)), col = c0 + cc;
+                float *dst = buf + (size_t)j * kTfCWP + cc;
+                if (col < nb)
+                    __pipeline_memcpy_async(dst, V + (long long)jl[j] * nb + col, 16);
+                else
+                    dst[0] = dst[1] = dst[2] = dst[3] = 0.f;
+            }
+        } else {
+            for (int idx = tid; idx < K * kTfCW; idx += kAbThreads) {
+                const int j = idx / kTfCW, cc = idx % kTfCW, col = c0 + cc;
+                float *dst = buf + (size_t)j * kTfCWP + cc;
+                if (col < nb)
+                    __pipeline_memcpy_async(dst, V + (long long)jl[j] * nb + col, 4);
+                else
+                    dst[0] = 0.f;
+            }
+        }
+        __pipeline_commit();
+    };
+    auto stage_l = [&](int c) {
+        const uint16_t *og = a.off + (size_t)c * a.offs;
+        for (int idx = tid; idx < a.offs / 8; idx += kAbThreads)
+            __pipeline_memcpy_async(os + 8 * idx, og + 8 * idx, 16);
+        const uint32_t b0 = a.base[c], n4 = (a.base[c + 1] - b0) / 4;
+        for (uint32_t idx = tid; idx < n4; idx += kAbThreads)
+            __pipeline_memcpy_async(es + 4 * idx, a.ent + b0 + 4 * idx, 16);
+        __pipeline_commit();
+    };
+    for (int Ia = blockIdx.x; Ia < a.na; Ia += gridDim.x) {
+        __syncthreads();
+        for (int idx = tid; idx < R16 * K8; idx += kAbThreads) {
+            const int m = idx / K8, j = idx - m * K8;
+            float v = 0.f;
+            if (j < K && m <= a.npair) {
+                const long long o = (long long)j * a.na + Ia;
+                v = m < a.npair ? a.m2[eri_index(a.fpA[o], m)] : a.a1A[o];
+                if (a.fsA[o] >> 31) v = -v;
+            }
+            As[(size_t)m * KP + j] = v;
+        }
+        for (int j = tid; j < K; j += kAbThreads)
+            jl[j] = (int)(a.fsA[(long long)j * a.na + Ia] & 0x3fffffffu);
+        float x[ITEMS];
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) x[i] = 0.f;
+        __syncthreads();
+        stage_b(0, Bs);
+        for (int ci = 0; ci < a.nchunk; ci++) {
+            const float *Bc = Bs + (size_t)(ci % NB) * K8 * kTfCWP;
+            __pipeline_wait_prior(0);
+            __syncthreads();
+            stage_l(ci);
+            const bool more = ci + 1 < a.nchunk;
+            if (NB == 2 && more) stage_b(ci + 1, Bs + (size_t)((ci + 1) & 1) * K8 * kTfCWP);
+            float acc[MT][2][4];
+#pragma unroll
+            for (int i = 0; i < MT; i++)
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) acc[i][j][q] = 0.f;
+            const float *ap = As + (size_t)(16 * wm * MT + g) * KP + t;
+            const float *bp = Bc + (size_t)t * kTfCWP + 16 * wn + g;
+#pragma unroll 2
+            for (int k0 = 0; k0 < K8; k0 += 8) {
+                uint32_t bh[2][2], bl[2][2];
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    split_tf32(bp[(size_t)k0 * kTfCWP + 8 * j], bh[j][0], bl[j][0]);
+                    split_tf32(bp[(size_t)(k0 + 4) * kTfCWP + 8 * j], bh[j][1], bl[j][1]);
+                }
+#pragma unroll
+                for (int i = 0; i < MT; i++) {
+                    const float *ar = ap + (size_t)16 * i * KP + k0;
+                    uint32_t ah[4], al[4];
+                    split_tf32(ar[0], ah[0], al[0]);
+                    split_tf32(ar[(size_t)8 * KP], ah[1], al[1]);
+                    split_tf32(ar[4], ah[2], al[2]);
+                    split_tf32(ar[(size_t)8 * KP + 4], ah[3], al[3]);
+#pragma unroll
+                    for (int j = 0; j < 2; j++) {
+                        mma_tf32(acc[i][j], al, bh[j][0], bh[j][1]);
+                        mma_tf32(acc[i][j], ah, bl[j][0], bl[j][1]);
+                        mma_tf32(acc[i][j], ah, bh[j][0], bh[j][1]);
+                    }
+                }
+            }
+            // fragments: lane holds rows g and g+8, columns 2t and 2t+1 of each tile
+#pragma unroll
+            for (int i = 0; i < MT; i++) {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int m = 16 * (wm * MT + i) + g + 8 * h;
+                    if (m < a.mrows) {
+#pragma unroll
+                        for (int j = 0; j < 2; j++) {
+                            float *dst = Ts + (size_t)m * kTfCW + 16 * wn + 8 * j + 2 * t;
+                            dst[0] = acc[i][j][2 * h];
+                            dst[1] = acc[i][j][2 * h + 1];
+                        }
+                    }
+                }
+            }
+            if (NB == 2 && more)
+                __pipeline_wait_prior(1);  // the lists (B chunk ci+1 may still fly)
+            else
+                __pipeline_wait_prior(0);
+            __syncthreads();
+            // single-buffered: chunk ci+1 is copied while chunk ci gathers
+            if (NB == 1 && more) stage_b(ci + 1, Bs);
+#pragma unroll
+            for (int i = 0; i < ITEMS; i++) {
+                const int Ib = tid + kAbThreads * i;
+                if (Ib < nb) {
+                    const int k1 = os[Ib + 1];
+                    float sacc = x[i];
+                    for (int k = os[Ib]; k < k1; k++) {
+                        const uint32_t e = es[k];
+                        const float v = Ts[(size_t)((e >> 8) & 0xffffu) * kTfCW + (e & 0xffu)];
+                        sacc += e >> 31 ? -v : v;
+                    }
+                    x[i] = sacc;
+                }
+            }
+        }
+        float *srow = S + (long long)Ia * nb;
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) {
+            const int Ib = tid + kAbThreads * i;
+            if (Ib < nb) srow[Ib] += x[i];
+        }
+    }
+}
+
 template <typename T>
 using AbKernel = void (*)(AbArgs<T>, const T *, T *);
 
@@ -381,6 +581,21 @@ AbKernel<double> dmma_kernel_mt(int mtw) {
     }
 }
 
+template <int ITEMS, int NB>
+AbKernel<float> tf32_kernel_mt(int mt) {
+    switch (mt) {
+        case 1: return k_sigma_ab_tf32<1, ITEMS, NB>;
+        case 2: return k_sigma_ab_tf32<2, ITEMS, NB>;
+        case 3: return k_sigma_ab_tf32<3, ITEMS, NB>;
+        case 4: return k_sigma_ab_tf32<4, ITEMS, NB>;
+        case 5: return k_sigma_ab_tf32<5, ITEMS, NB>;
+        default: return nullptr;
+    }
+}
+
+// 16-row tiles per warp of the TF32 engine (two warp rows)
+int tf_mt(int mrows) { return ((mrows + 15) / 16 + 1) / 2; }
+
 int ab_items(int nb) {
     const int it = (nb + kAbThreads - 1) / kAbThreads;
     return it <= 4 ? 4 : it <= 16 ? 16 : 0;
@@ -393,9 +608,19 @@ int dm_mtw(int mrows) { return ((mrows + 7) / 8 + 1) / 2; }
 
 // The tensor-core engine runs FP64 chunks of 64 columns (tx = 16).
 bool use_dmma(int tx, size_t w) { return tx == 16 && w == sizeof(double); }
+// In FP32, 64-column chunks (tx = 16) run 3xTF32 on the tensor cores.
+bool use_tf32(int tx, size_t w) { return tx == 16 && w == sizeof(float); }
 
 template <typename T>
 AbKernel<T> ab_kernel(int tx, int mrows, int items, int nbuf) {
+    if constexpr (sizeof(T) == sizeof(float)) {
+        if (use_tf32(tx, sizeof(T))) {
+            const int mt = tf_mt(mrows);
+            if (nbuf == 1)
+                return items == 4 ? tf32_kernel_mt<4, 1>(mt) : tf32_kernel_mt<16, 1>(mt);
+            return items == 4 ? tf32_kernel_mt<4, 2>(mt) : tf32_kernel_mt<16, 2>(mt);
+        }
+    }
     if constexpr (sizeof(T) == sizeof(double)) {
         if (use_dmma(tx, sizeof(T))) {
             const int mtw = dm_mtw(mrows);
@@ -422,6 +647,11 @@ int ab_maxent(const AbShape &sh, int cw) { return (cw * (1 + sh.nelb + sh.sb) + 
 // Dynamic shared memory of each engine; nbuf: B buffers of the tensor-core
 // engine; maxent, offs: longest chunk list and offset row stride.
 static size_t ab_smem_bytes(int tx, size_t w, int sa, int mrows, int nbuf, int maxent, int offs) {
+    if (use_tf32(tx, w)) {
+        const int K8 = tf_k8(sa), KP = tf_kp(sa), R16 = 32 * tf_mt(mrows);
+        return ((size_t)R16 * KP + (size_t)nbuf * K8 * kTfCWP + (size_t)mrows * kTfCW) * w +
+               (size_t)maxent * 4 + (size_t)offs * 2 + (size_t)sa * 4 + 16;
+    }
     if (use_dmma(tx, w)) {
         const int K4 = dm_k4(sa), KP = dm_kp(sa), R8 = 16 * dm_mtw(mrows);
         return ((size_t)R8 * KP + (size_t)nbuf * K4 * kDmCWP + (size_t)mrows * kDmCW) * w +
@@ -439,7 +669,9 @@ bool ab_possible(const AbShape &sh, int tx, size_t w, size_t smem_max) {
     const int mrows = sh.npair + 1;
     if (tx != 8 && tx != 16) return false;
     if (!ab_items(sh.nb) || sh.sa < 1 || mrows > 65535) return false;
-    if (use_dmma(tx, w)) {
+    if (use_tf32(tx, w)) {
+        if (tf_mt(mrows) > 5) return false;
+    } else if (use_dmma(tx, w)) {
         if (dm_mtw(mrows) > 9) return false;
     } else if (ab_tm(mrows, tx) > (tx == 16 ? 9 : 5)) {
         return false;
@@ -542,7 +774,7 @@ jci_status ab_launch(const AbArgs<T> &a, int tx, int device, const T *v, T *o,
     size_t smem = 0;
     int occ = 0, nsm = 0;
     for (int nbuf : {1, 2}) {
-        if (nbuf == 1 && !use_dmma(tx, sizeof(T))) continue;
+        if (nbuf == 1 && !use_dmma(tx, sizeof(T)) && !use_tf32(tx, sizeof(T))) continue;
         kern = ab_kernel<T>(tx, a.mrows, items, nbuf);
         if (!kern) return JCI_ERR_SPACE;
         smem = ab_smem_bytes(tx, sizeof(T), a.sa, a.mrows, nbuf, a.maxent, a.offs);
