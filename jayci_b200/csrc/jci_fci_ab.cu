@@ -382,15 +382,19 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-template <int MT, int ITEMS, int NB>
+// AS = 1: the A panel is split once per alpha string and kept as its TF32
+// parts (two panels); AS = 0: A is kept in FP32 and split at every load.
+template <int MT, int ITEMS, int NB, int AS>
 __global__ void __launch_bounds__(kAbThreads, NB == 1 ? 2 : 1)  // one B buffer: two CTAs per SM
     k_sigma_ab_tf32(AbArgs<float> a, const float *__restrict__ V, float *__restrict__ S) {
     if (a.skip && *a.skip) return;
     constexpr int R16 = 32 * MT;  // product rows covered (>= mrows)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int K = a.sa, K8 = tf_k8(K), KP = tf_kp(K), nb = a.nb;
-    float *As = reinterpret_cast<float *>(smem_raw);               // [R16][KP]
-    float *Bs = As + (size_t)R16 * KP;                             // [NB][K8][kTfCWP]
+    float *As = reinterpret_cast<float *>(smem_raw);               // [1 + AS][R16][KP]
+    uint32_t *Ah = reinterpret_cast<uint32_t *>(As);               // AS: TF32 high parts
+    uint32_t *Al = Ah + (size_t)R16 * KP;                          // AS: TF32 remainders
+    float *Bs = As + (size_t)(1 + AS) * R16 * KP;                  // [NB][K8][kTfCWP]
     float *Ts = Bs + NB * (size_t)K8 * kTfCWP;                     // [mrows][kTfCW]
     uint32_t *es = reinterpret_cast<uint32_t *>(Ts + (size_t)a.mrows * kTfCW);  // [maxent]
     uint16_t *os = reinterpret_cast<uint16_t *>(es + a.maxent);   // [offs]
@@ -444,7 +448,10 @@ __global__ void __launch_bounds__(kAbThreads, NB == 1 ? 2 : 1)  // one B buffer:
                 v = m < a.npair ? a.m2[eri_index(a.fpA[o], m)] : a.a1A[o];
                 if (a.fsA[o] >> 31) v = -v;
             }
-            As[(size_t)m * KP + j] = v;
+            if (AS)
+                split_tf32(v, Ah[(size_t)m * KP + j], Al[(size_t)m * KP + j]);
+            else
+                As[(size_t)m * KP + j] = v;
         }
         for (int j = tid; j < K; j += kAbThreads)
             jl[j] = (int)(a.fsA[(long long)j * a.na + Ia] & 0x3fffffffu);
@@ -467,7 +474,6 @@ __global__ void __launch_bounds__(kAbThreads, NB == 1 ? 2 : 1)  // one B buffer:
                 for (int j = 0; j < 2; j++)
 #pragma unroll
                     for (int q = 0; q < 4; q++) acc[i][j][q] = 0.f;
-            const float *ap = As + (size_t)(16 * wm * MT + g) * KP + t;
             const float *bp = Bc + (size_t)t * kTfCWP + 16 * wn + g;
 #pragma unroll 2
             for (int k0 = 0; k0 < K8; k0 += 8) {
@@ -479,12 +485,18 @@ __global__ void __launch_bounds__(kAbThreads, NB == 1 ? 2 : 1)  // one B buffer:
                 }
 #pragma unroll
                 for (int i = 0; i < MT; i++) {
-                    const float *ar = ap + (size_t)16 * i * KP + k0;
+                    const size_t ao = (size_t)(16 * (wm * MT + i) + g) * KP + t + k0;
+                    const size_t off[4] = {0, (size_t)8 * KP, 4, (size_t)8 * KP + 4};
                     uint32_t ah[4], al[4];
-                    split_tf32(ar[0], ah[0], al[0]);
-                    split_tf32(ar[(size_t)8 * KP], ah[1], al[1]);
-                    split_tf32(ar[4], ah[2], al[2]);
-                    split_tf32(ar[(size_t)8 * KP + 4], ah[3], al[3]);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        if (AS) {
+                            ah[q] = Ah[ao + off[q]];
+                            al[q] = Al[ao + off[q]];
+                        } else {
+                            split_tf32(As[ao + off[q]], ah[q], al[q]);
+                        }
+                    }
 #pragma unroll
                     for (int j = 0; j < 2; j++) {
                         mma_tf32(acc[i][j], al, bh[j][0], bh[j][1]);
@@ -581,14 +593,14 @@ AbKernel<double> dmma_kernel_mt(int mtw) {
     }
 }
 
-template <int ITEMS, int NB>
+template <int ITEMS, int NB, int AS>
 AbKernel<float> tf32_kernel_mt(int mt) {
     switch (mt) {
-        case 1: return k_sigma_ab_tf32<1, ITEMS, NB>;
-        case 2: return k_sigma_ab_tf32<2, ITEMS, NB>;
-        case 3: return k_sigma_ab_tf32<3, ITEMS, NB>;
-        case 4: return k_sigma_ab_tf32<4, ITEMS, NB>;
-        case 5: return k_sigma_ab_tf32<5, ITEMS, NB>;
+        case 1: return k_sigma_ab_tf32<1, ITEMS, NB, AS>;
+        case 2: return k_sigma_ab_tf32<2, ITEMS, NB, AS>;
+        case 3: return k_sigma_ab_tf32<3, ITEMS, NB, AS>;
+        case 4: return k_sigma_ab_tf32<4, ITEMS, NB, AS>;
+        case 5: return k_sigma_ab_tf32<5, ITEMS, NB, AS>;
         default: return nullptr;
     }
 }
@@ -615,10 +627,14 @@ template <typename T>
 AbKernel<T> ab_kernel(int tx, int mrows, int items, int nbuf) {
     if constexpr (sizeof(T) == sizeof(float)) {
         if (use_tf32(tx, sizeof(T))) {
+            // variant 3: one B buffer and the A panel pre-split; 1: one B
+            // buffer; 2: two B buffers
             const int mt = tf_mt(mrows);
+            if (nbuf == 3)
+                return items == 4 ? tf32_kernel_mt<4, 1, 1>(mt) : tf32_kernel_mt<16, 1, 1>(mt);
             if (nbuf == 1)
-                return items == 4 ? tf32_kernel_mt<4, 1>(mt) : tf32_kernel_mt<16, 1>(mt);
-            return items == 4 ? tf32_kernel_mt<4, 2>(mt) : tf32_kernel_mt<16, 2>(mt);
+                return items == 4 ? tf32_kernel_mt<4, 1, 0>(mt) : tf32_kernel_mt<16, 1, 0>(mt);
+            return items == 4 ? tf32_kernel_mt<4, 2, 0>(mt) : tf32_kernel_mt<16, 2, 0>(mt);
         }
     }
     if constexpr (sizeof(T) == sizeof(double)) {
@@ -648,8 +664,11 @@ int ab_maxent(const AbShape &sh, int cw) { return (cw * (1 + sh.nelb + sh.sb) + 
 // engine; maxent, offs: longest chunk list and offset row stride.
 static size_t ab_smem_bytes(int tx, size_t w, int sa, int mrows, int nbuf, int maxent, int offs) {
     if (use_tf32(tx, w)) {
+        // nbuf: the variant (3: one B buffer, A pre-split; 1: one B buffer; 2: two)
         const int K8 = tf_k8(sa), KP = tf_kp(sa), R16 = 32 * tf_mt(mrows);
-        return ((size_t)R16 * KP + (size_t)nbuf * K8 * kTfCWP + (size_t)mrows * kTfCW) * w +
+        const int apanels = nbuf == 3 ? 2 : 1, bbufs = nbuf == 2 ? 2 : 1;
+        return ((size_t)apanels * R16 * KP + (size_t)bbufs * K8 * kTfCWP +
+                (size_t)mrows * kTfCW) * w +
                (size_t)maxent * 4 + (size_t)offs * 2 + (size_t)sa * 4 + 16;
     }
     if (use_dmma(tx, w)) {
@@ -773,7 +792,8 @@ jci_status ab_launch(const AbArgs<T> &a, int tx, int device, const T *v, T *o,
     AbKernel<T> kern = nullptr;
     size_t smem = 0;
     int occ = 0, nsm = 0;
-    for (int nbuf : {1, 2}) {
+    for (int nbuf : {3, 1, 2}) {
+        if (nbuf == 3 && !use_tf32(tx, sizeof(T))) continue;
         if (nbuf == 1 && !use_dmma(tx, sizeof(T)) && !use_tf32(tx, sizeof(T))) continue;
         kern = ab_kernel<T>(tx, a.mrows, items, nbuf);
         if (!kern) return JCI_ERR_SPACE;
