@@ -163,7 +163,11 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def cpu_sample_plan(ndets, chunks=8, frac=0.25):
+def cpu_sample_plan(ndets, chunks=2, frac=0.25):
+    """Row blocks of the CPU sample.  Each call of the reference's kernel has a
+    fixed cost (about 50 ms here), which small blocks would charge to the
+    reference many times over; two blocks of 12.5% keep it under a few percent
+    of the timed work."""
     rows = max(1, int(ndets * frac / chunks))
     starts = [int((i + 0.5) * ndets / chunks - rows / 2) for i in range(chunks)]
     return [(max(0, min(ndets - rows - 1, s)), rows) for s in starts]
@@ -578,6 +582,10 @@ def run_profile(a):
 
 
 def main():
+    # the reference's sigma kernel runs its OpenMP loop with schedule(runtime):
+    # every CPU timing here uses all host threads and the same schedule
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    os.environ.setdefault("OMP_SCHEDULE", "dynamic,64")
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -588,7 +596,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-frac", type=float, default=0.25,
                     help="fraction of rows in the CPU-baseline sample (about 10 s)")
-    ap.add_argument("--ref-step-frac", type=float, default=0.02,
+    ap.add_argument("--ref-step-frac", type=float, default=0.25,
                     help="fraction of rows per step of --impl reference")
     ap.add_argument("--serve", type=int, default=0,
                     help="run the serving stream with this many requests instead")
