@@ -393,6 +393,15 @@ def run_gpu(a):
     return 0
 
 
+def serve_subspace(nroots):
+    """&dalginfo krymin, krymax of a serving request: a basis of 4 to 16 for
+    one or two roots, 8 to 24 for three or four.  Collapsing to only the
+    roots' own Ritz vectors (krymin = nroots) loses the thick restart: a
+    4-root CAS(12,12) solve takes 2289 iterations at 4 / 16 and 767 at
+    8 / 24."""
+    return (4, 16) if nroots <= 2 else (8, 24)
+
+
 def run_serve(a):
     """Serving stream: CAS(m,m) solves, m uniform in {6, 8, 10, 12}, 1-4 roots,
     chained in 32-step geometry scans (base integrals seed 105 + scan, each
@@ -435,11 +444,13 @@ def run_serve(a):
         pos[sc] += 1
     N = len(seq)
     prec = jb.MIXED if a.serve_mixed else jb.FP64
-    kw = dict(krymin=4, krymax=16, refdim=8, restol=1e-8, maxiter=5000, precision=prec)
+    kw = dict(refdim=8, restol=1e-8, maxiter=5000, precision=prec)
 
     def submit(srv, r, warm):
+        kmin, kmax = serve_subspace(r["nroots"])
         return srv.submit((r["m"], r["m"], 0, 0, r["m"], 0, 0), r["m1"], r["m2"], r["e_nuc"],
-                          0.0, nroots=r["nroots"], warm_from=warm, **kw)
+                          0.0, nroots=r["nroots"], warm_from=warm, krymin=kmin, krymax=kmax,
+                          **kw)
 
     def by_size(rows):
         out = {}
@@ -470,7 +481,8 @@ def run_serve(a):
         sp = spaces[m]
         ts = time.perf_counter()
         sp.set_integrals(r["m1"], r["m2"], r["e_nuc"], 0.0)
-        res = sp.davidson(maxiter=5000, krymin=4, krymax=16, nroots=r["nroots"], refdim=8,
+        kmin, kmax = serve_subspace(r["nroots"])
+        res = sp.davidson(maxiter=5000, krymin=kmin, krymax=kmax, nroots=r["nroots"], refdim=8,
                           restol=1e-8, want_vectors=False)
         rows.append((m, time.perf_counter() - ts, res.stats.iterations,
                      res.stats.sigma_seconds))
