@@ -644,7 +644,7 @@ __global__ void __launch_bounds__(ITEMS * RB <= 4 ? 1024 : 512)
     }
 }
 
-// ---- streaming plan (mode 3) ----------------------------------------------
+// ---- streaming plans (modes 3, 4; the beta singles of modes 6, 7) ----------
 //
 // Every term whose coefficient is the same for a whole row runs as row
 // streams: the diagonal and the alpha doubles on C (rows Ia), and the beta
@@ -654,8 +654,10 @@ __global__ void __launch_bounds__(ITEMS * RB <= 4 ? 1024 : 512)
 // whole source row, coalesced, from L2 (the vector stays resident), and no
 // per-element excitation table is read.  The beta part is added back to
 // sigma with a tiled transpose; the alpha singles and alpha x beta doubles
-// come from k_sigma_mixed as in plan 1.  Every sigma element is still
-// summed in a fixed order.
+// come from a product kernel (k_sigma_mixed or k_sigma_ab).  Modes 6 and 7
+// keep only the beta singles here and take the doubles by string groups
+// (jci_fci_group.cu).  Every sigma element is still summed in a fixed
+// order.
 
 constexpr int kTile = 32;
 
