@@ -105,12 +105,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def committed_traffic(workload):
-    """Per-launch DRAM bytes of the sigma kernel from the committed ncu summary."""
+def committed_traffic(workload, mode):
+    """Per-launch DRAM bytes of sigma plan `mode` on `workload` from the
+    committed ncu summary (one entry per captured plan), or None when that
+    plan was not captured."""
     p = os.path.join(ROOT, "profiles", f"sigma_{workload}_traffic.json")
     if os.path.exists(p):
         try:
-            return json.load(open(p)).get("dram_bytes_per_launch")
+            plan = json.load(open(p)).get("plans", {}).get(str(mode))
+            return plan.get("dram_bytes_per_launch") if plan else None
         except Exception:
             return None
     return None
@@ -335,7 +338,8 @@ def run_gpu(a):
     avg_launch_s = statistics.mean(launches) / 1e3
     peak, peak_kind = measured_peaks()
     achieved = bytes_per_launch / avg_launch_s / 1e9
-    traffic = committed_traffic(a.workload)
+    mode, nt, R, B, _ = sp.sigma_tuning(jb.FP64)
+    traffic = committed_traffic(a.workload, mode)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic,
             "algorithmic_bytes_per_launch": bytes_per_launch, "peak_source": peak_kind,
@@ -369,7 +373,6 @@ def run_gpu(a):
                    "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"reference sigma (compute_cblock_Hfastest), {nvec} vectors, "
                              f"{sample}, OMP_SCHEDULE=dynamic,64"}
-    mode, nt, R, B, _ = sp.sigma_tuning(jb.FP64)
     out = {"metric": METRIC, "value": value, "unit": "Gdet/s", "n_gpus": world,
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": tot_ms / a.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
