@@ -47,7 +47,7 @@ WORKLOADS = {
 }
 # &dalginfo per workload: krymin, krymax, refdim, maxiter (restol 1e-8)
 DALGINFO = {"cas10_10": (4, 12, 8, 500), "fci12_12": (6, 24, 12, 500),
-            "fci14_14_fc2": (8, 24, 16, 2000), "fci16_16": (4, 12, 8, 500)}
+            "fci14_14_fc2": (8, 48, 16, 2000), "fci16_16": (4, 12, 8, 500)}
 METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"] \
     if os.path.exists(os.path.join(ROOT, "BASELINE.json")) else "sigma-build Gdet/s"
 
