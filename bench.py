@@ -75,8 +75,11 @@ def sigma_plan_desc(mode, nt, R, B):
           else "row_kernel_threads"): nt,
          ("staged_rows" if mode == 0 else
           "product_column_threads" if mode in (4, 5, 7) else "product_ctas_per_sm"): R}
-    d["beta_pass_threads" if streams else "group_columns_per_thread" if groups
-      else "rows_per_cta"] = B
+    if groups:
+        d["group_kernel"] = (f"{B} column(s) per thread" if B <= 2 else
+                             f"targets split over 4 warps, {5 - B} column(s) per lane")
+    else:
+        d["beta_pass_threads" if streams else "rows_per_cta"] = B
     return d
 
 

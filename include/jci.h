@@ -198,8 +198,10 @@ jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sigma,
  * SM, 0 = as many as fit; modes 4, 5, 7: column threads of the fused
  * product, 8 (CUDA cores, 32-column chunks) or 16 (tensor cores, 64-column
  * chunks: FP64 mma.sync in FP64, 3xTF32 in FP32)), `batch` (modes 1, 2, 5: alpha strings per CTA of the
- * row kernel; modes 3-4: threads per CTA of the beta pass; modes 6-7:
- * columns per thread of the group kernel, 1 or 2), and its timed cost in
+ * row kernel; modes 3-4: threads per CTA of the beta pass; modes 6-7: the
+ * group kernel variant, 1 or 2 columns per thread, or 3, 4: the group's
+ * excitation targets split over 4 warps with 2 or 1 columns per lane), and
+ * its timed cost in
  * ms per vector.  All 0 before the first sigma call and on the
  * multi-group path.  No reference counterpart (the reference has no device
  * tuning). */

@@ -240,7 +240,7 @@ class Space:
         return m.value, a.value, b.value, g.value, c.value
 
     def set_sigma_plan(self, precision, mode, threads, rows=1, batch=1):
-        """Fix the FCI sigma plan (modes 0-5 of jci_sigma_set_plan)."""
+        """Fix the FCI sigma plan (modes 0-7 of jci_sigma_set_plan)."""
         _check(lib().jci_sigma_set_plan(self.h, precision, mode, threads, rows, batch),
                "sigma_set_plan")
 

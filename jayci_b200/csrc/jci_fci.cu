@@ -1138,7 +1138,8 @@ static jci_status group_tables(jci_space *s, cudaStream_t st) {
 static bool group_possible(const FciTables *f) { return f->da >= 1 && f->db >= 1; }
 
 // Doubles of spin sp by groups: rows x len matrix x -> y (add: y += ...),
-// with the diagonal hd when given; items = columns per thread (1 or 2).
+// with the diagonal hd when given; items = the group kernel variant (1-4,
+// group_launch).
 template <typename T>
 static jci_status launch_group(jci_space *s, int sp, const T *hd, int add, const int *skip,
                                int items, const T *x, T *y, cudaStream_t st) {
@@ -1397,7 +1398,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
             if (ms < bs) { bs = ms; b6s = nt; }
         }
         float gg = 1e30f;
-        for (int it : {1, 2}) {
+        for (int it : {1, 2, 3, 4}) {
             float ms = timeit([&] {
                 jci_status q = launch_group<T>(s, 1, nullptr, 1, nullptr, it, ct, tau, st);
                 return q ? q : launch_group<T>(s, 0, a.hd, 0, nullptr, it, v, o, st);
@@ -1425,10 +1426,10 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     if (b3a && b3b)
         best3 = best_of([&] { return run_plan<T>(s, a, smode, b3a, sR, b3b, v, o, st); });
     if (best6 < 1e30f) {
-        // both column counts of the group kernel, end to end (their
-        // component timings are close and noisy)
+        // every group kernel variant, end to end (their component timings
+        // are close and noisy)
         best6 = 1e30f;
-        for (int it : {1, 2}) {
+        for (int it : {1, 2, 3, 4}) {
             float ms = best_of([&] { return run_plan<T>(s, a, gmode, b6s, sR, it, v, o, st); });
             if (ms < best6) { best6 = ms; b6i = it; }
         }
@@ -1537,7 +1538,7 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, 
     size_t w = p ? sizeof(float) : sizeof(double);
     if (mode == 6 || mode == 7) {
         bool ok = mode == 6 ? mixed_possible(f, w) && R >= 0 : ab_plan_possible(f, R, w);
-        if (!ok || !group_possible(f) || !stream_ok(f->na, nt) || (B != 1 && B != 2) ||
+        if (!ok || !group_possible(f) || !stream_ok(f->na, nt) || B < 1 || B > 4 ||
             stream_smem(0, f->sb, w) > f->smem_max)
             return JCI_ERR_ARG;
     } else if (mode == 3 || mode == 4) {

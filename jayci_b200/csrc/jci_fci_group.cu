@@ -42,8 +42,9 @@ constexpr int kGroupChunk = 64;  // union entries per staged chunk
 // The entries k0..k1-1 of the staged chunk (coefficient rows cs, source
 // rows js) that belong to class QM: reached only by the row quads set in
 // QM (bit q: rows 4q..4q+3), so the FMAs of the other quads, whose
-// coefficients are all zero, are not issued.  k1 - k0 is a multiple of 4.
-template <typename T, int ITEMS, int QM>
+// coefficients are all zero, are not issued.  k0 and k1 are multiples of
+// 4; the caller takes every STRIDE-th entry quad from k0 (STRIDE 1: all).
+template <typename T, int ITEMS, int QM, int STRIDE = 1>
 __device__ __forceinline__ void group_class(T (&acc)[kGroupRows][ITEMS],
                                             const T *__restrict__ X,
                                             const T (*__restrict__ cs)[kGroupRows],
@@ -52,7 +53,7 @@ __device__ __forceinline__ void group_class(T (&acc)[kGroupRows][ITEMS],
     using V = typename Vec16<T>::type;
     constexpr int E = 16 / (int)sizeof(T);  // rows per 16-byte piece
     constexpr int QE = 4 / E;               // pieces per row quad
-    for (int k = k0; k < k1; k += 4) {
+    for (int k = k0; k < k1; k += 4 * STRIDE) {
         T x[4][ITEMS];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
@@ -170,6 +171,110 @@ __global__ void __launch_bounds__(NT, 512 / NT)  // at least 16 warps per SM
                 Y[o + col[i]] = v;
             }
         }
+    }
+}
+
+// The same sums for small spaces, where one thread per column leaves the
+// SMs nearly idle (FCI(12,12): 58 groups x 4 segments of 256 columns).
+// Here the W warps of a CTA share its 32 ITEMS columns (lane + 32 i) and
+// split the group's union: within every staged chunk, warp w takes the
+// entry quads whose index in the chunk is w mod W.  The W partial sums of
+// each output are then added in shared memory in warp order, so results
+// stay bitwise reproducible.
+constexpr int kSplitWarps = 4;
+
+template <typename T, int ITEMS>
+__global__ void __launch_bounds__(32 * kSplitWarps)
+    k_sigma_group_split(GroupArgs<T> a, const T *__restrict__ X, T *__restrict__ Y) {
+    if (a.skip && *a.skip) return;
+    constexpr int RG = kGroupRows, W = kSplitWarps, NT = 32 * W, CW = 32 * ITEMS;
+    constexpr size_t kStage = 2 * kGroupChunk * RG * sizeof(T) + 2 * kGroupChunk * sizeof(int);
+    constexpr size_t kRed = (size_t)W * RG * CW * sizeof(T);
+    __shared__ __align__(16) unsigned char smem[kStage > kRed ? kStage : kRed];
+    __shared__ int sg[17];
+    T(*cs)[kGroupChunk][RG] = reinterpret_cast<T(*)[kGroupChunk][RG]>(smem);
+    int(*js)[kGroupChunk] =
+        reinterpret_cast<int(*)[kGroupChunk]>(smem + 2 * kGroupChunk * RG * sizeof(T));
+    T *red = reinterpret_cast<T *>(smem);  // [W][RG][CW], after the last chunk
+    const int g = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int len = a.len, r0 = g * RG, nr = min(RG, a.rows - r0);
+    const int c0 = blockIdx.y * CW;
+    const int u0 = a.uoff[g], u1 = a.uoff[g + 1];
+    if (tid < 17) sg[tid] = a.useg[(size_t)g * 17 + tid];
+    auto stage = [&](int u, int b) {
+        const int n = min(kGroupChunk, u1 - u);
+        constexpr int per = RG * (int)sizeof(T) / 16;
+        for (int idx = tid; idx < n * per; idx += NT)
+            __pipeline_memcpy_async(reinterpret_cast<char *>(&cs[b][0][0]) + 16 * idx,
+                                    reinterpret_cast<const char *>(a.coef + (size_t)u * RG) +
+                                        16 * idx,
+                                    16);
+        for (int idx = tid; idx < n; idx += NT) js[b][idx] = a.uidx[u + idx];
+        __pipeline_commit();
+    };
+    T acc[RG][ITEMS];
+#pragma unroll
+    for (int r = 0; r < RG; r++)
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) acc[r][i] = T(0);
+    int col[ITEMS];
+    bool in[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; i++) {
+        col[i] = c0 + lane + 32 * i;
+        in[i] = col[i] < len;
+    }
+    if (u0 < u1) stage(u0, 0);
+    int b = 0;
+    for (int u = u0; u < u1; u += kGroupChunk, b ^= 1) {
+        __pipeline_wait_prior(0);
+        __syncthreads();  // chunk b landed; every thread is done with chunk b^1
+        if (u + kGroupChunk < u1) stage(u + kGroupChunk, b ^ 1);
+        const int ue = min(u + kGroupChunk, u1);
+        // class QM's part of the chunk, [lo, hi) relative to u: this warp's
+        // first quad is the first one at or after lo with index = warp mod W
+#define JCI_CLASS(QM)                                                                  \
+    {                                                                                  \
+        const int lo = max(sg[QM], u) - u, hi = min(sg[QM + 1], ue) - u;               \
+        if (lo < hi) {                                                                 \
+            const int k0 = lo + 4 * ((warp - (lo >> 2) % W + W) % W);                   \
+            if (k0 < hi)                                                               \
+                group_class<T, ITEMS, QM, W>(acc, X, cs[b], js[b], col, in, len, k0, hi); \
+        }                                                                              \
+    }
+        JCI_CLASS(1)
+        JCI_CLASS(2)
+        JCI_CLASS(3)
+        JCI_CLASS(4)
+        JCI_CLASS(5)
+        JCI_CLASS(6)
+        JCI_CLASS(7)
+        JCI_CLASS(8)
+        JCI_CLASS(9)
+        JCI_CLASS(10)
+        JCI_CLASS(11)
+        JCI_CLASS(12)
+        JCI_CLASS(13)
+        JCI_CLASS(14)
+        JCI_CLASS(15)
+#undef JCI_CLASS
+    }
+    __syncthreads();  // the staging buffers become the reduction buffer
+#pragma unroll
+    for (int r = 0; r < RG; r++)
+#pragma unroll
+        for (int i = 0; i < ITEMS; i++) red[((size_t)warp * RG + r) * CW + lane + 32 * i] = acc[r][i];
+    __syncthreads();
+    for (int idx = tid; idx < RG * CW; idx += NT) {
+        const int r = idx / CW, cc = idx - r * CW, c = c0 + cc;
+        if (r >= nr || c >= len) continue;
+        T v = red[idx];
+#pragma unroll
+        for (int w = 1; w < W; w++) v += red[(size_t)w * RG * CW + idx];
+        const long long o = (long long)(r0 + r) * len + c;
+        if (a.hd) v = fma(a.hd[o], X[o], v);
+        if (a.add) v += Y[o];
+        Y[o] = v;
     }
 }
 
@@ -298,12 +403,25 @@ jci_status group_fill(GroupTables *t, const double *dblH, const float *dblHf, cu
     return JCI_OK;
 }
 
-// 256-thread CTAs (256 ITEMS columns each), or 128-thread ones when the
-// wider CTAs would give fewer than four per SM (small spaces).
+// Variants 1 and 2: one thread per column with `variant` columns each, in
+// 256-thread CTAs, or 128-thread ones when the wider CTAs would give fewer
+// than four per SM.  Variants 3 and 4: the union split over the warps of a
+// CTA (k_sigma_group_split) with 2 and 1 columns per lane.
 template <typename T>
-jci_status group_launch(const GroupArgs<T> &a, int items, int device, const T *x, T *y,
+jci_status group_launch(const GroupArgs<T> &a, int variant, int device, const T *x, T *y,
                         cudaStream_t st) {
-    if (items != 1 && items != 2) return JCI_ERR_ARG;
+    if (variant < 1 || variant > 4) return JCI_ERR_ARG;
+    if (variant >= 3) {
+        const int ng = (a.rows + kGroupRows - 1) / kGroupRows, cw = variant == 3 ? 64 : 32;
+        const dim3 grid(ng, (a.len + cw - 1) / cw);
+        if (variant == 3)
+            k_sigma_group_split<T, 2><<<grid, 32 * kSplitWarps, 0, st>>>(a, x, y);
+        else
+            k_sigma_group_split<T, 1><<<grid, 32 * kSplitWarps, 0, st>>>(a, x, y);
+        JCI_CUDA(cudaGetLastError());
+        return JCI_OK;
+    }
+    const int items = variant;
     int nsm = 0;
     JCI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     const int ng = (a.rows + kGroupRows - 1) / kGroupRows;

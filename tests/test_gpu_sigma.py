@@ -85,8 +85,9 @@ def test_sigma_against_oracle(gen):
                                   (2, 512, 2, 1), (2, 128, 0, 4), (3, 128, 1, 128),
                                   (3, 256, 0, 512), (3, 1024, 2, 256), (4, 256, 8, 256),
                                   (4, 128, 16, 512), (5, 256, 8, 2), (5, 128, 16, 1),
-                                  (6, 128, 0, 1), (6, 256, 2, 2), (7, 128, 8, 2),
-                                  (7, 256, 16, 1)])
+                                  (6, 128, 0, 1), (6, 256, 2, 2), (6, 128, 0, 3),
+                                  (6, 256, 1, 4), (7, 128, 8, 2), (7, 256, 16, 1),
+                                  (7, 256, 16, 3), (7, 128, 8, 4)])
 @pytest.mark.parametrize("prec", [jb.FP64, jb.FP32])
 def test_every_fci_plan(name, plan, prec):
     """Each launch plan the autotuner may pick gives the reference's sigma."""
@@ -107,8 +108,9 @@ def test_every_fci_plan(name, plan, prec):
 def test_fused_product_and_groups_wide_rows(prec):
     """CAS(12e,14o), 3003 x 3003 strings: the fused product (16 strings per
     thread in the gather, 94 or 47 column chunks) and the string-group
-    doubles (several column segments per row) give the sigma of the panel
-    plan, whose parity with the reference is tested above."""
+    doubles (several column segments per row; the union split over warps
+    in variants 3 and 4) give the sigma of the panel plan, whose parity with
+    the reference is tested above."""
     s = jb.Space(12, 14)
     ints = make_integrals(14, 14, 5)
     m1, m2 = ints.packed()
@@ -117,7 +119,8 @@ def test_fused_product_and_groups_wide_rows(prec):
     s.set_sigma_plan(prec, 3, 256, 0, 256)
     ref = s.sigma(V, prec)
     tol = 1e-12 if prec == jb.FP64 else 5e-6  # two FP32 sums in different orders
-    for plan in ((4, 256, 8, 256), (4, 256, 16, 256), (6, 256, 0, 1), (7, 256, 16, 2)):
+    for plan in ((4, 256, 8, 256), (4, 256, 16, 256), (6, 256, 0, 1), (7, 256, 16, 2),
+                 (6, 256, 0, 3), (7, 256, 16, 4)):
         s.set_sigma_plan(prec, *plan)
         got = s.sigma(V, prec)
         assert np.abs(got - ref).max() <= tol * np.abs(ref).max()
