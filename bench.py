@@ -108,14 +108,16 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def committed_traffic(workload, mode):
+def committed_traffic(workload, mode, B):
     """Per-launch DRAM bytes of sigma plan `mode` on `workload` from the
-    committed ncu summary (one entry per captured plan), or None when that
-    plan was not captured."""
+    committed ncu summary, or None when that plan was not captured.  Entries
+    are keyed by mode, and for the string-group plans (6, 7) by mode and
+    group kernel variant ("7:3")."""
+    key = f"{mode}:{B}" if mode in (6, 7) else str(mode)
     p = os.path.join(ROOT, "profiles", f"sigma_{workload}_traffic.json")
     if os.path.exists(p):
         try:
-            plan = json.load(open(p)).get("plans", {}).get(str(mode))
+            plan = json.load(open(p)).get("plans", {}).get(key)
             return plan.get("dram_bytes_per_launch") if plan else None
         except Exception:
             return None
@@ -342,7 +344,7 @@ def run_gpu(a):
     peak, peak_kind = measured_peaks()
     achieved = bytes_per_launch / avg_launch_s / 1e9
     mode, nt, R, B, _ = sp.sigma_tuning(jb.FP64)
-    traffic = committed_traffic(a.workload, mode)
+    traffic = committed_traffic(a.workload, mode, B)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic,
             "algorithmic_bytes_per_launch": bytes_per_launch, "peak_source": peak_kind,
