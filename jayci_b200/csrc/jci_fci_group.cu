@@ -184,8 +184,8 @@ __global__ void __launch_bounds__(NT, 512 / NT)  // at least 16 warps per SM
 constexpr int kSplitWarps = 4;
 
 template <typename T, int ITEMS>
-__global__ void __launch_bounds__(32 * kSplitWarps)
-    k_sigma_group_split(GroupArgs<T> a, const T *__restrict__ X, T *__restrict__ Y) {
+__device__ __forceinline__ void group_split(const GroupArgs<T> &a, const T *__restrict__ X,
+                                            T *__restrict__ Y) {
     if (a.skip && *a.skip) return;
     constexpr int RG = kGroupRows, W = kSplitWarps, NT = 32 * W, CW = 32 * ITEMS;
     constexpr size_t kStage = 2 * kGroupChunk * RG * sizeof(T) + 2 * kGroupChunk * sizeof(int);
@@ -276,6 +276,22 @@ __global__ void __launch_bounds__(32 * kSplitWarps)
         if (a.add) v += Y[o];
         Y[o] = v;
     }
+}
+
+// Register bounds: the FP64 2-column form takes 136 registers unbounded (3
+// CTAs per SM) and fits 128 without spills at 4 CTAs per SM.  The other
+// forms keep the compiler's own choice: any bound there makes it spend
+// registers on unrolling and lose occupancy (FP32 2-column: 66 unbounded,
+// 96 or spills when bounded).
+template <typename T, int ITEMS>
+__global__ void __launch_bounds__(32 * kSplitWarps)
+    k_sigma_group_split(GroupArgs<T> a, const T *__restrict__ X, T *__restrict__ Y) {
+    group_split<T, ITEMS>(a, X, Y);
+}
+__global__ void __launch_bounds__(32 * kSplitWarps, 4)
+    k_sigma_group_split_f64x2(GroupArgs<double> a, const double *__restrict__ X,
+                              double *__restrict__ Y) {
+    group_split<double, 2>(a, X, Y);
 }
 
 // coef[(uoff[g] + upos[f][s]) RG + s - g RG] = dblH[f][s] for every double f
@@ -414,9 +430,14 @@ jci_status group_launch(const GroupArgs<T> &a, int variant, int device, const T 
     if (variant >= 3) {
         const int ng = (a.rows + kGroupRows - 1) / kGroupRows, cw = variant == 3 ? 64 : 32;
         const dim3 grid(ng, (a.len + cw - 1) / cw);
-        if (variant == 3)
-            k_sigma_group_split<T, 2><<<grid, 32 * kSplitWarps, 0, st>>>(a, x, y);
-        else
+        if constexpr (sizeof(T) == sizeof(double)) {
+            if (variant == 3)
+                k_sigma_group_split_f64x2<<<grid, 32 * kSplitWarps, 0, st>>>(a, x, y);
+        } else {
+            if (variant == 3)
+                k_sigma_group_split<T, 2><<<grid, 32 * kSplitWarps, 0, st>>>(a, x, y);
+        }
+        if (variant == 4)
             k_sigma_group_split<T, 1><<<grid, 32 * kSplitWarps, 0, st>>>(a, x, y);
         JCI_CUDA(cudaGetLastError());
         return JCI_OK;
