@@ -1,0 +1,48 @@
+"""Host-side pieces of bench.py's JSON line: the roofline traffic comes from
+the committed ncu capture of the plan that actually ran, and the plan
+description names each plan's own parameters."""
+import json
+import os
+
+import bench
+
+
+def test_traffic_is_looked_up_per_plan_and_group_variant():
+    # FCI(12,12): plan 5 and plan 7 with group variants 2 and 3 were captured
+    assert bench.committed_traffic("fci12_12", 5, 1) > 0
+    assert bench.committed_traffic("fci12_12", 7, 3) > 0
+    assert bench.committed_traffic("fci12_12", 7, 2) > 0
+    # plans or variants without a capture report no traffic
+    assert bench.committed_traffic("fci12_12", 7, 4) is None
+    assert bench.committed_traffic("fci12_12", 1, 1) is None
+    assert bench.committed_traffic("fci14_14_fc2", 6, 2) > 0
+    assert bench.committed_traffic("fci14_14_fc2", 6, 3) is None
+    assert bench.committed_traffic("no_such_workload", 5, 1) is None
+
+
+def test_every_traffic_entry_points_at_a_committed_summary():
+    prof = os.path.join(bench.ROOT, "profiles")
+    for name in os.listdir(prof):
+        if not name.endswith("_traffic.json"):
+            continue
+        d = json.load(open(os.path.join(prof, name)))
+        assert d["plans"]
+        for key, plan in d["plans"].items():
+            mode = int(key.split(":")[0])
+            assert mode in bench.PLAN_NAMES
+            assert (":" in key) == (mode in (6, 7))   # group plans carry their variant
+            assert plan["dram_bytes_per_launch"] > 0 and plan["kernels"]
+            assert os.path.exists(os.path.join(bench.ROOT, plan["summary"]))
+
+
+def test_plan_description_names_each_plans_parameters():
+    d = bench.sigma_plan_desc(7, 512, 16, 3)
+    assert d["beta_singles_threads"] == 512 and d["product_column_threads"] == 16
+    assert "split over 4 warps, 2 column" in d["group_kernel"]
+    assert "1 column" in bench.sigma_plan_desc(6, 256, 0, 1)["group_kernel"]
+    assert "split over 4 warps, 1 column" in bench.sigma_plan_desc(6, 256, 0, 4)["group_kernel"]
+    d = bench.sigma_plan_desc(3, 256, 0, 512)
+    assert d["alpha_pass_threads"] == 256 and d["beta_pass_threads"] == 512
+    d = bench.sigma_plan_desc(5, 256, 16, 2)
+    assert d["row_kernel_threads"] == 256 and d["rows_per_cta"] == 2
+    assert set(bench.SIGMA_KERNELS) == set(bench.PLAN_NAMES) == set(range(8))
