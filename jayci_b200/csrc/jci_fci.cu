@@ -1208,9 +1208,11 @@ static jci_status launch_transposes(const FciTables *f, const T *v, T *ct, T *o,
 // modes 3, 4: row streams on C^T (B threads) and C (nt threads), then the
 //   product: 3: k_sigma_mixed (R CTAs per SM), 4: k_sigma_ab (R column
 //   threads).
-// modes 6, 7: the same-spin doubles by string groups on C and C^T (B
-//   columns per thread), the beta singles as a row stream on C^T (nt
-//   threads), then the product of mode 3 (6) or of mode 4 (7).
+// modes 6, 7: the same-spin doubles by string groups on C and C^T (group
+//   kernel variant B: 1 or 2 columns per thread, or 3, 4: the union split
+//   over 4 warps with 2 or 1 columns per lane), the beta singles as a row
+//   stream on C^T (nt threads), then the product of mode 3 (6) or of
+//   mode 4 (7).
 template <typename T>
 static jci_status run_plan(jci_space *s, FciArgs<T> a, int mode, int nt, int R, int B,
                            const T *v, T *o, cudaStream_t st) {
