@@ -124,6 +124,25 @@ def committed_traffic(workload, mode, B):
     return None
 
 
+def committed_tensor_pipe(workload):
+    """Tensor-pipe utilisation of the kernels that use the tensor cores on
+    `workload`, from the committed ncu captures, or None when there is none.
+    ncu cannot run inside a timed bench, so these figures are quoted from
+    the captures, each with the summary that holds its command."""
+    p = os.path.join(ROOT, "profiles", f"tensor_pipe_{workload}.json")
+    if os.path.exists(p):
+        try:
+            d = json.load(open(p))
+            return {"source": d["note"],
+                    "kernels": [{k: e[k] for k in ("kernel", "use", "pipe", "active_pct",
+                                                   "useful_fraction_of_tile", "summary")
+                                 if k in e}
+                                for e in d["kernels"]]}
+        except Exception:
+            return None
+    return None
+
+
 class ClockSampler:
     """SM clock and throttle-reason sampling during the timed region: NVML
     (the library nvidia-smi reads) polled from a thread every 2 ms, so short
@@ -393,6 +412,9 @@ def run_gpu(a):
            "clocks": clk,
            "fp32_sigma_gdet_s": value32,
            "solves": solves}
+    tp = committed_tensor_pipe(a.workload)
+    if tp:
+        out["tensor_pipe"] = tp
     if rank == 0:
         print(json.dumps(out))
     if dist:

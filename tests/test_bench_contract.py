@@ -46,3 +46,14 @@ def test_plan_description_names_each_plans_parameters():
     d = bench.sigma_plan_desc(5, 256, 16, 2)
     assert d["row_kernel_threads"] == 256 and d["rows_per_cta"] == 2
     assert set(bench.SIGMA_KERNELS) == set(bench.PLAN_NAMES) == set(range(8))
+
+
+def test_tensor_pipe_figures_come_from_committed_captures():
+    tp = bench.committed_tensor_pipe("fci12_12")
+    assert "not measured in the run" in tp["source"]
+    names = [k["kernel"] for k in tp["kernels"]]
+    assert any(n.startswith("k_gram") for n in names)
+    for k in tp["kernels"]:
+        assert 0 < k["active_pct"] <= 100
+        assert os.path.exists(os.path.join(bench.ROOT, k["summary"]))
+    assert bench.committed_tensor_pipe("cas10_10") is None
