@@ -82,3 +82,21 @@ def test_space_limits_rejected():
     assert ei.value.status == 2
     with pytest.raises(jb.JciError):
         jb.Space(10, 70, 0, 0, 70)  # 70 internal orbitals > 64
+
+
+def test_sigma_plan_calls_checked_on_the_host():
+    """jci_sigma_set_plan refuses bad modes and precisions (JCI_ERR_ARG) and
+    any plan before jci_set_integrals (JCI_ERR_STATE); jci_sigma_tuning
+    reports zeros before the first sigma.  No device is touched."""
+    s = jb.Space(6, 6)
+    for args in ((jb.FP64, 8, 256, 1, 1), (jb.FP64, -1, 256, 1, 1),
+                 (jb.MIXED, 1, 256, 1, 1), (7, 1, 256, 1, 1)):
+        with pytest.raises(jb.JciError) as ei:
+            s.set_sigma_plan(*args)
+        assert ei.value.status == 1
+    with pytest.raises(jb.JciError) as ei:
+        s.set_sigma_plan(jb.FP64, 7, 256, 16, 3)
+    assert ei.value.status == 12
+    assert s.sigma_tuning(jb.FP64) == (0, 0, 0, 0, 0.0)
+    assert s.sigma_tuning(jb.FP32) == (0, 0, 0, 0, 0.0)
+    s.close()
