@@ -172,12 +172,22 @@ jci_status jci_sigma_device(jci_space *s, int nvec, const void *v,
  * keeps its per-CTA panels in a fixed device array of 64 MiB that lives in
  * the library (every GPU that loads libjci holds it until exit) instead of
  * a buffer allocated on first use; jci_set_integrals must have been called
- * before (it builds the tables this call reads).  One-group (FCI / CAS)
- * spaces only; returns JCI_ERR_SPACE when one alpha row's panel,
- * (n(n+1)/2 + 1) x Nbeta rounded up to 64 elements, exceeds 64 MiB.  The
- * first call on a device looks up the array's device address (once per
- * device, with that device current); make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (other
+ * before (it builds the tables this call reads).  Returns JCI_ERR_SPACE,
+ * before launching anything, for any space outside these limits:
+ *   - one occupation group per spin (FCI / CAS / DOCC+ACTV with xlevel 0);
+ *   - n(n+1)/2 + 1 <= 144 for n CI orbitals (n <= 16), the product
+ *     kernel's row tile;
+ *   - the product kernel's shared memory, Nsingles_alpha x (16 TM + 128)
+ *     elements with TM = ceil((n(n+1)/2 + 1) / 16), fits the device's
+ *     opt-in limit;
+ *   - one alpha row's panel, (n(n+1)/2 + 1) x Nbeta rounded up to 64
+ *     elements, fits in 64 MiB;
+ *   - the row kernel holds one beta row in shared memory and at most 32
+ *     columns per thread (Nbeta <= 16384).
+ * The call makes the space's device current.  The first call on a device
+ * looks up the array's device address (once per device, made current for
+ * the lookup); make that first call before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU (other
  * streams, other host threads, other handles on the same device) race and
  * must be serialised by the caller.  Nothing in the array needs clearing: a
  * call writes every panel element before reading it.  No counterpart in the

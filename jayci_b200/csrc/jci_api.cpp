@@ -138,6 +138,7 @@ jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sig, int 
     if (!s || !v || !sig) return JCI_ERR_ARG;
     if (precision != JCI_FP64 && precision != JCI_FP32) return JCI_ERR_ARG;
     if (!s->have_ints || !s->dev) return JCI_ERR_STATE;
+    if (cudaSetDevice(s->dev->device) != cudaSuccess) return JCI_ERR_CUDA;
     cudaStream_t st = stream ? (cudaStream_t)stream : s->dev->stream;
     return fci_sigma_noalloc(s, v, sig, precision, st);
 }

@@ -1596,13 +1596,23 @@ static void *g_noalloc_ptr[kMaxDevices];
 static std::once_flag g_noalloc_once[kMaxDevices];
 static cudaError_t g_noalloc_err[kMaxDevices];
 
-// Device address of g_noalloc_scratch on the current device.  The host-side
-// name is only a stand-in for the symbol, so the address is looked up once
-// per device (with that device current) and cached.
+// Device address of g_noalloc_scratch on device `dev`.  The host-side name
+// is only a stand-in for the symbol, so the address is looked up once per
+// device, with that device made current for the lookup (the caller's
+// current device is restored afterwards), and cached.
 static jci_status noalloc_scratch(int dev, void **out) {
     if (dev < 0 || dev >= kMaxDevices) return JCI_ERR_ARG;
     std::call_once(g_noalloc_once[dev], [dev]() {
-        g_noalloc_err[dev] = cudaGetSymbolAddress(&g_noalloc_ptr[dev], g_noalloc_scratch);
+        int prev = -1;
+        cudaError_t e = cudaGetDevice(&prev);
+        if (e == cudaSuccess && prev != dev) e = cudaSetDevice(dev);
+        if (e == cudaSuccess)
+            e = cudaGetSymbolAddress(&g_noalloc_ptr[dev], g_noalloc_scratch);
+        if (prev >= 0 && prev != dev) {
+            cudaError_t e2 = cudaSetDevice(prev);
+            if (e == cudaSuccess) e = e2;
+        }
+        g_noalloc_err[dev] = e;
     });
     if (g_noalloc_err[dev] != cudaSuccess)
         return cuda_fail(g_noalloc_err[dev], "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__,
@@ -1652,9 +1662,20 @@ static jci_status sigma_noalloc(jci_space *s, const T *v, T *o, cudaStream_t st)
     void *scratch = nullptr;
     jci_status r = noalloc_scratch(d->device, &scratch);
     if (r) return r;
-    // row kernel: the tuned thread count if there is one, else a fixed shape
-    int nt = f->tuned_nt[prec] ? f->tuned_nt[prec] : (a.nb > 2048 ? 512 : 256);
-    if ((r = launch_one<T>(a, nt, fci_smem(a.nb, a.npair, 0, w), a.na, v, o, st))) return r;
+    // Row kernel k_sigma_fci.  The tuned thread count is a k_sigma_fci shape
+    // only when the autotuner picked mode 0; every other mode's count belongs
+    // to another kernel, so a fixed shape is used then.  Either way the
+    // shape is checked as fci_force_plan checks mode 0 before anything runs.
+    int nt = f->tuned_mode[prec] == 0 && f->tuned_nt[prec] ? f->tuned_nt[prec]
+                                                           : (a.nb > 2048 ? 512 : 256);
+    int items = (a.nb + nt - 1) / nt;
+    if ((nt != 128 && nt != 256 && nt != 512 && nt != 1024) || items > 32 ||
+        (nt == 1024 && items > 2))
+        return JCI_ERR_SPACE;
+    size_t row_smem = fci_smem(a.nb, a.npair, 0, w);
+    if (row_smem > f->smem_max) return JCI_ERR_SPACE;
+    if ((r = launch_one<T>(a, nt, row_smem, a.na, v, o, st))) return r;
+    JCI_CUDA(cudaGetLastError());  // the product adds into the row kernel's output
     size_t smem = mix_smem(m.sa, TM, w);
     JCI_CUDA(smem_optin(kern));
     int occ = 0, nsm = 0;

@@ -7,8 +7,9 @@ allocation after start-up.  For them libjci offers a sigma whose scratch
 panels live in a fixed 64 MiB device array inside the library.  This file
 checks it through the C ABI against the ordinary entry point
 (jci_sigma_device) on two consecutive calls, with the same tolerances as the
-other sigma tests (FP64 1e-12, FP32 2e-6 of max|sigma|).  It is named so that
-pytest collects it last.
+other sigma tests (FP64 1e-12, FP32 2e-6 of max|sigma|), and checks that the
+device's free memory does not move across its first call on a fresh space.
+It is named so that pytest collects it last.
 """
 import ctypes
 import os
@@ -22,6 +23,7 @@ from jayci_b200.synth import make_integrals
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TOL = {jb.FP64: 1e-12, jb.FP32: 2e-6}
 
 
 def _space(name):
@@ -32,12 +34,42 @@ def _space(name):
     return s, g
 
 
+def _cas(n, seed):
+    """CAS(n, n) with nalpha = nbeta: one occupation group per spin."""
+    s = jb.Space(n, n)
+    ints = make_integrals(n, n, seed)
+    m1, m2 = ints.packed()
+    s.set_integrals(m1, m2, ints.e_nuc, 0.0)
+    return s
+
+
 def _noalloc(s, v_ptr, o_ptr, prec, stream):
     f = jb.lib().jci_sigma_device_noalloc
     f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                   ctypes.c_void_p]
     return f(s.h, ctypes.c_void_p(v_ptr), ctypes.c_void_p(o_ptr), prec,
              ctypes.c_void_p(stream))
+
+
+def _vector(n, prec, seed):
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    dt = torch.float64 if prec == jb.FP64 else torch.float32
+    return torch.randn(n, dtype=torch.float64, device="cuda", generator=g).to(dt)
+
+
+def _check_two_calls(s, v, ref, prec, stream):
+    """Two noalloc calls in a row into NaN-filled outputs, each against ref."""
+    import torch
+    tol = TOL[prec] * ref.abs().max().item()
+    out = None
+    for _ in range(2):  # consecutive calls share the static scratch array
+        out = torch.full_like(v, float("nan"))
+        assert _noalloc(s, v.data_ptr(), out.data_ptr(), prec, stream) == 0
+        torch.cuda.synchronize()
+        assert not torch.isnan(out).any().item()
+        assert (out - ref).abs().max().item() <= tol
+    return out
 
 
 @pytest.mark.parametrize("name", ["cas10_10", "cas7_7"])
@@ -52,14 +84,80 @@ def test_noalloc_matches_sigma_device(name, prec):
         ref = torch.empty_like(v)
         s.sigma_device(v.data_ptr(), ref.data_ptr(), 1, s.ndets, prec, st.cuda_stream)
         torch.cuda.synchronize()
-        tol = (1e-12 if prec == jb.FP64 else 2e-6) * ref.abs().max().item()
-        for _ in range(2):  # two calls in a row share the static scratch array
-            out = torch.full_like(v, float("nan"))
-            assert _noalloc(s, v.data_ptr(), out.data_ptr(), prec, st.cuda_stream) == 0
-            torch.cuda.synchronize()
-            assert (out - ref).abs().max().item() <= tol
+        out = _check_two_calls(s, v, ref, prec, st.cuda_stream)
     golden = g["sigma"][0]
+    tol = TOL[prec] * np.abs(golden).max()
     assert np.abs(out.double().cpu().numpy() - golden).max() <= 2 * tol
+
+
+# CAS(10,10), FCI(12e,12o) (853 776 determinants) and FCI(14e,14o) (11 778 624
+# determinants, Nbeta = 3432 > 2048: the row kernel's wider default shape)
+@pytest.mark.parametrize("n", [10, 12, 14])
+@pytest.mark.parametrize("prec", [jb.FP64, jb.FP32])
+def test_noalloc_first_call_allocates_nothing(n, prec):
+    """The noalloc call is the first sigma on a freshly built space; device
+    free memory is read before and after it.  A space of the same shape is
+    run first so that the kernels this shape uses are already loaded (the
+    CUDA runtime loads a kernel's code on its first launch, which is the
+    library's code, not an allocation made by the call)."""
+    import torch
+    warm = _cas(n, 1)
+    wv = _vector(warm.ndets, prec, 5)
+    wo = torch.empty_like(wv)
+    assert _noalloc(warm, wv.data_ptr(), wo.data_ptr(), prec, 0) == 0
+    torch.cuda.synchronize()
+    del wv, wo
+    warm.close()
+
+    s = _cas(n, 2)
+    v = _vector(s.ndets, prec, 6)
+    out = torch.full_like(v, float("nan"))
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    rc = _noalloc(s, v.data_ptr(), out.data_ptr(), prec, 0)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert rc == 0
+    assert free1 == free0, f"free device memory moved by {free0 - free1} bytes"
+    ref = torch.empty_like(v)
+    s.sigma_device(v.data_ptr(), ref.data_ptr(), 1, s.ndets, prec, 0)
+    torch.cuda.synchronize()
+    tol = TOL[prec] * ref.abs().max().item()
+    assert (out - ref).abs().max().item() <= tol
+    _check_two_calls(s, v, ref, prec, 0)
+    s.close()
+
+
+# (mode, threads, rows, batch) as jci_sigma_set_plan takes them, with the edge
+# thread counts of each kernel; the noalloc call must pick its own row-kernel
+# shape whatever plan the space was left with
+PLANS = [(0, 128, 2, 1), (0, 512, 4, 1), (1, 128, 0, 1), (1, 1024, 0, 1), (2, 256, 0, 2),
+         (3, 128, 0, 1024), (3, 1024, 0, 128), (4, 512, 16, 512), (5, 256, 8, 1),
+         (6, 128, 0, 2), (6, 1024, 0, 1), (7, 512, 16, 3), (7, 128, 8, 4)]
+
+
+@pytest.mark.parametrize("prec", [jb.FP64, jb.FP32])
+def test_noalloc_after_every_forced_plan(prec):
+    """FCI(14e,14o): every admissible forced plan, then noalloc against
+    jci_sigma_device under that plan."""
+    import torch
+    s = _cas(14, 3)
+    v = _vector(s.ndets, prec, 9)
+    ref = torch.empty_like(v)
+    ran = 0
+    for mode, nt, rows, batch in PLANS:
+        try:
+            s.set_sigma_plan(prec, mode, nt, rows, batch)
+        except jb.JciError as e:
+            assert e.status == 1, (mode, nt, rows, batch, e)
+            continue
+        ref.fill_(float("nan"))
+        s.sigma_device(v.data_ptr(), ref.data_ptr(), 1, s.ndets, prec, 0)
+        torch.cuda.synchronize()
+        _check_two_calls(s, v, ref, prec, 0)
+        ran += 1
+    assert ran >= 10
+    s.close()
 
 
 def test_noalloc_rejects_unsupported_space():
