@@ -31,9 +31,24 @@ def _ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+REF_ENV = "JAYCI_REF"
+
+
+def reference_tree():
+    """The reference checkout named by the JAYCI_REF environment variable
+    (the directory holding mpi_source/), or None when it is unset or absent."""
+    root = os.environ.get(REF_ENV)
+    if root and os.path.isfile(os.path.join(root, "mpi_source", "pdavidson.c")):
+        return root
+    return None
+
+
 def build(ref: bool = True) -> None:
-    """Compile the oracle libraries (make -C oracle)."""
-    target = ["all"] if ref else ["liboracle.so"]
+    """Compile the oracle libraries (make -C oracle): always the C
+    restatement; with ref=True also the reference build, from the tree
+    reference_tree() names (skipped when there is none)."""
+    root = reference_tree() if ref else None
+    target = ["all", f"REF={root}"] if root else ["liboracle.so"]
     subprocess.run(["make", "-s", "-C", HERE] + target, check=True)
 
 
@@ -136,6 +151,19 @@ class OracleSpace:
         S = np.zeros_like(V)
         self.lib().jo_sigma(self.h, _ptr(m1), _ptr(m2), V.shape[0], _ptr(V), _ptr(S))
         return S
+
+    def sigma_rows(self, m1, m2, v, rows):
+        """(H v)[rows] for one vector v (ndets) at the listed determinants."""
+        lib = self.lib()
+        lib.jo_sigma_rows.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_longlong,
+                                                              ctypes.c_void_p]
+        v = np.ascontiguousarray(v, float)
+        rows = np.ascontiguousarray(rows, np.int64)
+        out = np.zeros(len(rows))
+        lib.jo_sigma_rows(self.h, _ptr(np.ascontiguousarray(m1, float)),
+                          _ptr(np.ascontiguousarray(m2, float)), _ptr(v), _ptr(rows),
+                          len(rows), _ptr(out))
+        return out
 
     def davidson(self, m1, m2, totcore, maxiter=500, krymin=4, krymax=12,
                  nroots=1, prediagr=1, refdim=8, restol=1e-8, init=None):
