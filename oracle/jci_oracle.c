@@ -590,15 +590,47 @@ void jo_sigma(const jo_space *s, const double *m1, const double *m2,
         jo_sigma_range(s, m1, m2, nvec, V, S, 0, s->ndets);
 }
 
+/* One sigma row d of nvec vectors into acc[nvec]: the full-row gather of
+ * <d|H|j> v_j over every determinant j that differs from d by a single or
+ * double replacement (pdavidson.c:1867 compute_hij_eosp and its evaluators
+ * :2892-3655, written as a gather instead of the reference's upper-triangle
+ * scatter). */
+static void sigma_row(const jo_space *s, const double *m1, const double *m2,
+                      int nvec, const double *V, long long d, double *acc);
+
 void jo_sigma_range(const jo_space *s, const double *m1, const double *m2,
                     int nvec, const double *V, double *S, long long d0,
                     long long d1)
 {
-        const struct jo_spin *A = &s->sp[0], *B = &s->sp[1];
-        int na = A->nelec, nb = B->nelec;
         long long N = s->ndets;
         double *acc = malloc(sizeof(double) * nvec);
         for (long long d = d0; d < d1 && d < N; d++) {
+                sigma_row(s, m1, m2, nvec, V, d, acc);
+                for (int v = 0; v < nvec; v++) S[v * N + d] = acc[v];
+        }
+        free(acc);
+}
+
+void jo_sigma_rows(const jo_space *s, const double *m1, const double *m2,
+                   const double *V, const long long *rows, long long nrows,
+                   double *out)
+{
+        for (long long r = 0; r < nrows; r++) {
+                if (rows[r] < 0 || rows[r] >= s->ndets) {
+                        out[r] = 0.0;
+                        continue;
+                }
+                sigma_row(s, m1, m2, 1, V, rows[r], &out[r]);
+        }
+}
+
+static void sigma_row(const jo_space *s, const double *m1, const double *m2,
+                      int nvec, const double *V, long long d, double *acc)
+{
+        const struct jo_spin *A = &s->sp[0], *B = &s->sp[1];
+        int na = A->nelec, nb = B->nelec;
+        long long N = s->ndets;
+        {
                 int k, p, q;
                 det_strings(s, d, &k, &p, &q);
                 const int *sa = A->istr + (long long)p * na;
@@ -647,9 +679,7 @@ void jo_sigma_range(const jo_space *s, const double *m1, const double *m2,
                         double h = h2aa(g->io0, g->io1, g->fo0, g->fo1, g->sign, m2);
                         for (int v = 0; v < nvec; v++) acc[v] += h * V[v * N + j];
                 }
-                for (int v = 0; v < nvec; v++) S[v * N + d] = acc[v];
         }
-        free(acc);
 }
 
 /* ---- dense eigensolver ------------------------------------------- */

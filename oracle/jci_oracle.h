@@ -55,6 +55,12 @@ void jo_sigma_range(const jo_space *s, const double *m1, const double *m2,
                     int nvec, const double *V, double *S, long long d0,
                     long long d1);
 
+/* Sigma of one vector V (ndets) at the determinants rows[0..nrows) only:
+ * out[r] = (H V)[rows[r]] (out-of-range rows give 0). */
+void jo_sigma_rows(const jo_space *s, const double *m1, const double *m2,
+                   const double *V, const long long *rows, long long nrows,
+                   double *out);
+
 /* Root-sequential Davidson (pdavidson.c:39).  Returns iterations taken
  * (>= 0) or a negative error.  energies[nroots] include totcore; civec is
  * nroots x ndets.  init (prediagr=3) supplies krymin start vectors. */

@@ -243,7 +243,8 @@ void ref_sigma(double *m1, double *m2, int nvec, const double *V, double *C)
 }
 
 /* Bounded samples of the reference's sigma for CPU timing: ref_sigma_prepare
- * sets up V, C, D and W once; ref_sigma_rows_timed runs the reference's
+ * sets up V, C, D (<i|H|i>, compute_diagonal_iHi) and W once;
+ * ref_sigma_rows_timed runs the reference's
  * row-range kernel compute_cblock_Hfastest (pdavidson.c:1296) for rows
  * [row0, row0 + nrows) of the upper triangle and returns its wall time in
  * seconds (setup excluded).  The partial C it accumulates is not a sigma. */
@@ -263,6 +264,9 @@ int ref_sigma_prepare(double *m1, double *m2, int nvec, const double *V)
         T_nvec = nvec;
         T_m1 = m1;
         T_m2 = m2;
+        compute_diagonal_iHi(shim_ga_data(T_d), 0, S.ndets - 1, m1, m2,
+                             S.ci_aelec, S.ci_belec, S.intorb, T_w, S.pstr,
+                             S.qstr);
         memcpy(shim_ga_data(T_v), V, sizeof(double) * nvec * S.ndets);
         return 0;
 }
@@ -289,6 +293,28 @@ double ref_sigma_rows_timed(int row0, int nrows)
         free(cdata);
         deallocate_mem_cont_int(&wi, widata);
         return (b.tv_sec - a.tv_sec) + 1e-9 * (b.tv_nsec - a.tv_nsec);
+}
+
+/* One timed step of the reference's sigma on rows [row0, row0 + nrows) of
+ * every vector: the diagonal term sigma = D o v that perform_hvispacefast
+ * applies first (compute_hvc_diagonal_ga, pdavidson.c:2105, whose
+ * GA_Elem_multiply_patch is restricted here to the same rows), then
+ * compute_cblock_Hfastest on those rows (pdavidson.c:1296).  Returns the
+ * wall time of both in seconds; *diag_s receives the diagonal part. */
+double ref_sigma_step_timed(int row0, int nrows, double *diag_s)
+{
+        struct timespec a, b;
+        clock_gettime(CLOCK_MONOTONIC, &a);
+        for (int k = 0; k < T_nvec; k++) {
+                int d_lo[1] = {row0}, d_hi[1] = {row0 + nrows - 1};
+                int p_lo[2] = {k, row0}, p_hi[2] = {k, row0 + nrows - 1};
+                GA_Elem_multiply_patch(T_d, d_lo, d_hi, T_v, p_lo, p_hi, T_c, p_lo,
+                                       p_hi);
+        }
+        clock_gettime(CLOCK_MONOTONIC, &b);
+        double t_diag = (b.tv_sec - a.tv_sec) + 1e-9 * (b.tv_nsec - a.tv_nsec);
+        if (diag_s) *diag_s = t_diag;
+        return t_diag + ref_sigma_rows_timed(row0, nrows);
 }
 
 void ref_sigma_release(void) { shim_ga_reset(); }

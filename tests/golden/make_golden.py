@@ -8,7 +8,8 @@ yij/cij tables, excitation lists, <i|H|i>, sigma on seeded random vectors,
 Davidson energies / vectors, and Dyson orbitals between (N+1)- and
 N-electron wavefunctions.
 
-    OMP_NUM_THREADS=1 python tests/golden/make_golden.py
+    JAYCI_REF=<reference checkout> OMP_NUM_THREADS=1 python tests/golden/make_golden.py
+    python tests/golden/make_golden.py fci12_12 fci14_14_fc2 fci16_16
 
 Only this script touches the reference; the tests read the .npz files.
 """
@@ -133,6 +134,76 @@ def make_dyson(name):
     print(name, vecs[0].shape, vecs[1].shape, np.abs(dy).max())
 
 
+# Bench-size workloads (jayci_b200.synth.WORKLOADS), written as
+# bench_<workload>.npz: full vectors do not fit in the repository, so these
+# fixtures hold samples.  Input vectors are the
+# counter-hash vectors of seeded.py, which the tests regenerate.
+#   fci12_12      the reference's own sigma (full, then sampled) and the
+#                 reference's own pdavidson with the bench's &dalginfo
+#                 (krymin 6, krymax 24, refdim 12, 3 roots, restol 1e-8);
+#   fci14_14_fc2, fci16_16
+#                 sigma at sampled rows from the oracle's row gather
+#                 (jo_sigma_rows), whose agreement with the reference's own
+#                 sigma is pinned on the fci12_12 rows by the CPU tests.
+SIGMA_SEED, PROJ_SEEDS, ROW_SEED, NROWS = 1, (1001, 1002, 1003, 1004), 7, 4096
+TOPK = 2048
+
+
+def _projections(x, n):
+    from seeded import hash_vector
+    return np.array([hash_vector(n, s) @ x for s in PROJ_SEEDS])
+
+
+def make_large(name, davidson=True):
+    from seeded import hash_vector, sample_rows
+
+    from jayci_b200.synth import WORKLOADS, workload_integrals
+    from oracle.oracle import OracleSpace
+    w = WORKLOADS[name]
+    ints = workload_integrals(name)
+    m1, m2 = ints.packed()
+    n, k = w["n"], w["k"]
+    out = dict(general=np.array([2 * k + 2 * w["nfrozen"], n + w["nfrozen"], w["nfrozen"],
+                                 0, n, 0, 0]),
+               m1_sum=m1.sum(), m2_sum=m2.sum(), e_nuc=ints.e_nuc, e_fc=ints.e_fc,
+               sigma_seed=SIGMA_SEED, proj_seeds=np.array(PROJ_SEEDS))
+    if name == "fci12_12":
+        ref = RefSpace(2 * k, n)
+        N = ref.ndets
+        v = hash_vector(N, SIGMA_SEED)
+        S = ref.sigma(m1, m2, v)[0]
+        rows = sample_rows(N, NROWS, ROW_SEED)
+        out.update(ndets=N, rows=rows, sigma_rows=S[rows], sigma_norm2=S @ S,
+                   sigma_proj=_projections(S, N), source="reference")
+        if davidson:
+            kmin, kmax, refdim, nroots = 6, 24, 12, 3
+            civ, _ = ref.davidson(m1, m2, ints.e_nuc, 0.0, maxiter=500, krymin=kmin,
+                                  krymax=kmax, nroots=nroots, prediagr=1, refdim=refdim,
+                                  restol=1e-8)
+            Sc = ref.sigma(m1, m2, civ)
+            e = np.einsum("ij,ij->i", civ, Sc) + ints.e_nuc
+            top = np.argsort(-np.abs(civ), axis=1)[:, :TOPK]
+            out.update(dav_opts=np.array([kmin, kmax, nroots, refdim]), energies=e,
+                       civec_idx=top, civec_val=np.take_along_axis(civ, top, axis=1),
+                       civec_proj=np.array([_projections(c, N) for c in civ]),
+                       civec_res=np.linalg.norm(Sc - (e - ints.e_nuc)[:, None] * civ, axis=1))
+    else:
+        o = OracleSpace(k, k, n)
+        N = o.ndets
+        v = hash_vector(N, SIGMA_SEED)
+        rows = sample_rows(N, NROWS, ROW_SEED)
+        out.update(ndets=N, rows=rows, sigma_rows=o.sigma_rows(m1, m2, v, rows),
+                   source="oracle")
+    np.savez_compressed(os.path.join(HERE, f"bench_{name}.npz"), **out)
+    print(name, out["ndets"], out.get("energies"))
+
+
 if __name__ == "__main__":
+    sys.path.insert(0, HERE)
     for n in (sys.argv[1:] or list(CASES) + list(DYSON_CASES)):
-        (make_dyson if n in DYSON_CASES else make)(n)
+        if n in DYSON_CASES:
+            make_dyson(n)
+        elif n in CASES:
+            make(n)
+        else:
+            make_large(n)

@@ -17,7 +17,7 @@ from oracle.oracle import OracleSpace
 pytestmark = pytest.mark.gpu
 
 GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
-                if not os.path.basename(p).startswith("dyson_"))
+                if not os.path.basename(p).startswith(("dyson_", "bench_")))
 NAMES = [os.path.basename(p)[:-4] for p in GOLDEN]
 
 
