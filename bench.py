@@ -1,29 +1,33 @@
 #!/usr/bin/env python
 """bench.py -- sigma-build throughput of the determinant-CI hot path.
 
-Workload (default): FCI(12e,12o), 924 x 924 = 853 776 determinants, the
-3-root configuration, seeded synthetic integrals (rank 12, seed 102) -- the
-largest named configuration the metric is quoted on that fits one GPU run of
-a few seconds.  A step is one sigma = H c build for a block of 3 vectors (one
-per root) in FP64 with every input resident in HBM; the L2 (126 MB) is
-flushed by writing a 256 MiB buffer before every step because the vectors
-and tables would otherwise stay L2-resident.
+Workload (default): FCI(16e,16o), 12 870 x 12 870 = 165 636 900
+determinants, 1 root, seeded synthetic integrals (rank 16, seed 104): the
+largest configuration of the metric that one GPU holds.  A step is one
+sigma = H c build of one vector (the root count) in FP64 with every input
+resident in HBM.  The vectors (1.33 GB) are far larger than the 126 MB L2;
+a 256 MiB write still flushes it before every step.
 
 value  = determinants x vectors / sigma time  (Gdet/s, all ranks)
 e2e    = the same through the public C ABI (jci_sigma) from pinned host
-         buffers, host->device copy of the 3 input vectors and device->host
-         copy of the 3 sigma vectors inside every timed step
-Extra fields report the FP32 sigma rate and full Davidson solves (plain
-FP64 reference schedule vs the mixed FP32->FP64 two-phase schedule,
-energies compared) measured outside the timed region.
+         buffers, host->device copy of the input vector and device->host
+         copy of the sigma vector inside every timed step
+Extra keys (outside the timed region): the FP32 sigma rate; the one-time
+setup costs (host string tables, device tables, the sigma autotuner's
+first call); and the full Davidson solve pair of FCI(14e,14o) with two
+frozen-core orbitals, 4 roots -- the plain FP64 reference schedule against
+the mixed FP32 -> FP64 schedule, each after an untimed warm-up solve.
 
 --impl reference times the reference's own CPU code (oracle/_ref, the
 reference's mpi_source compiled unchanged against a single-process GA/MPI
-stand-in) on the same workload: each step runs the reference's sigma
-kernel compute_cblock_Hfastest with all host threads over a fixed sample of
-rows spread evenly across the determinant list and extrapolates to the full
-sigma.  Multi-GPU runs (torchrun) are replicas: every rank builds the same
-workload independently (weak scaling); no data-path collective exists.
+stand-in) on the same workload with every usable host thread: each step is
+the reference's sigma (the diagonal term, pdavidson.c:2105, then
+compute_cblock_Hfastest, pdavidson.c:1296) on one contiguous block of rows.
+ms_per_step is the time of that block; the rows, their fraction of a full
+sigma, the reference's fixed cost per call and the full-sigma time
+extrapolated from the two are separate keys.  Multi-GPU runs (torchrun)
+are replicas: every rank builds the same workload independently (weak
+scaling); no data-path collective exists.
 """
 from __future__ import annotations
 
@@ -31,7 +35,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import time
 
@@ -48,6 +51,9 @@ WORKLOADS = {
 # &dalginfo per workload: krymin, krymax, refdim, maxiter (restol 1e-8)
 DALGINFO = {"cas10_10": (4, 12, 8, 500), "fci12_12": (6, 24, 12, 500),
             "fci14_14_fc2": (8, 48, 16, 2000), "fci16_16": (4, 12, 8, 500)}
+# the solve pair reported beside each sigma workload
+SOLVES_OF = {"fci16_16": "fci14_14_fc2", "fci14_14_fc2": "fci14_14_fc2",
+             "fci12_12": "fci12_12", "cas10_10": "cas10_10"}
 METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"] \
     if os.path.exists(os.path.join(ROOT, "BASELINE.json")) else "sigma-build Gdet/s"
 
@@ -68,7 +74,7 @@ PLAN_NAMES = {0: "staged rows", 1: "row kernel, dense product through a global p
               7: "string-group doubles, beta-singles stream, fused product and gather"}
 
 
-def sigma_plan_desc(mode, nt, R, B):
+def sigma_plan_desc(mode, nt, R, B, ms=None):
     streams, groups = mode in (3, 4), mode in (6, 7)
     d = {"mode": mode, "name": PLAN_NAMES[mode],
          ("alpha_pass_threads" if streams else "beta_singles_threads" if groups
@@ -80,6 +86,8 @@ def sigma_plan_desc(mode, nt, R, B):
                              f"targets split over 4 warps, {5 - B} column(s) per lane")
     else:
         d["beta_pass_threads" if streams else "rows_per_cta"] = B
+    if ms is not None:
+        d["autotuner_ms_per_vector"] = ms
     return d
 
 
@@ -108,17 +116,16 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def committed_traffic(workload, mode, B):
-    """Per-launch DRAM bytes of sigma plan `mode` on `workload` from the
-    committed ncu summary, or None when that plan was not captured.  Entries
-    are keyed by mode, and for the string-group plans (6, 7) by mode and
-    group kernel variant ("7:3")."""
+def committed_profile(workload, mode, B):
+    """Per-launch figures of sigma plan `mode` on `workload` from the
+    committed ncu summary (profiles/sigma_<workload>_traffic.json), or None
+    when that plan was not captured.  Entries are keyed by mode, and for
+    the string-group plans (6, 7) by mode and group kernel variant ("7:3")."""
     key = f"{mode}:{B}" if mode in (6, 7) else str(mode)
     p = os.path.join(ROOT, "profiles", f"sigma_{workload}_traffic.json")
     if os.path.exists(p):
         try:
-            plan = json.load(open(p)).get("plans", {}).get(key)
-            return plan.get("dram_bytes_per_launch") if plan else None
+            return json.load(open(p)).get("plans", {}).get(key)
         except Exception:
             return None
     return None
@@ -190,78 +197,207 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def cpu_sample_plan(ndets, chunks=2, frac=0.25):
-    """Row blocks of the CPU sample.  Each call of the reference's kernel has a
-    fixed cost (about 50 ms here), which small blocks would charge to the
-    reference many times over; two blocks of 12.5% keep it under a few percent
-    of the timed work."""
-    rows = max(1, int(ndets * frac / chunks))
-    starts = [int((i + 0.5) * ndets / chunks - rows / 2) for i in range(chunks)]
-    return [(max(0, min(ndets - rows - 1, s)), rows) for s in starts]
+# ---- the reference's own sigma on the host cores ---------------------------
+
+def host_threads(ndets, nvec):
+    """Host threads for the reference's sigma: every core, bounded by memory.
+    compute_hij_eosp keeps a private full-length sigma buffer per OpenMP
+    thread (pdavidson.c:1930-2078), nvec x ndets doubles each, beside
+    about 5 x that of shared arrays (V, C, D, W and the row buffers)."""
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        return cores
+    try:  # a cgroup limit below the machine's memory
+        lim = open("/sys/fs/cgroup/memory.max").read().strip()
+        if lim != "max":
+            avail = min(avail, int(lim))
+    except Exception:
+        pass
+    per = 8.0 * nvec * ndets
+    fit = int((0.8 * avail - 6 * per) // per)
+    return max(1, min(cores, fit))
 
 
-def reference_sigma_sample(name, nvec, frac=0.25):
-    """Time the reference's own sigma kernel on an even row sample; returns
-    (extrapolated seconds for a full sigma of nvec vectors, sample string)."""
-    import ctypes
+class RefSigma:
+    """The reference's sigma (oracle/_ref) prepared once on one workload;
+    step(rows) times one contiguous row block at a rotating position."""
 
-    import numpy as np
+    def __init__(self, name, nvec):
+        import ctypes
 
-    from jayci_b200.synth import workload_integrals
-    from oracle.oracle import RefSpace, _ptr, ref_available
-    if not ref_available():
-        return None, "reference build absent"
-    (e, o, nfc), _, _, _ = WORKLOADS[name]
-    ints = workload_integrals(name)
-    m1, m2 = ints.packed()
-    ref = RefSpace(e, o, nfc)
-    L = ref.lib()
-    L.ref_sigma_rows_timed.restype = ctypes.c_double
-    V = np.random.default_rng(0).standard_normal((nvec, ref.ndets))
-    L.ref_sigma_prepare(_ptr(m1), _ptr(m2), nvec, _ptr(V))
-    plan = cpu_sample_plan(ref.ndets, frac=frac)
-    t = sum(L.ref_sigma_rows_timed(r0, nr) for r0, nr in plan)
-    rows = sum(nr for _, nr in plan)
-    L.ref_sigma_release()
-    return t * ref.ndets / rows, f"{len(plan)} evenly spaced row blocks, {rows} of {ref.ndets} rows"
+        import numpy as np
+
+        from jayci_b200.synth import workload_integrals
+        from oracle.oracle import RefSpace, _ptr
+        (e, o, nfc), _, _, _ = WORKLOADS[name]
+        ints = workload_integrals(name)
+        self.m1, self.m2 = ints.packed()
+        self.ref = RefSpace(e, o, nfc)
+        self.ndets, self.nvec = self.ref.ndets, nvec
+        L = self.ref.lib()
+        L.ref_sigma_step_timed.restype = ctypes.c_double
+        L.ref_sigma_step_timed.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        V = np.random.default_rng(0).standard_normal((nvec, self.ndets))
+        L.ref_sigma_prepare(_ptr(self.m1), _ptr(self.m2), nvec, _ptr(V))
+        del V
+        self.L, self.k = L, 0
+
+    def step(self, rows):
+        import ctypes
+        rows = max(1, min(int(rows), self.ndets))
+        # block positions walk through the determinant list (golden ratio)
+        frac = (self.k * 0.6180339887498949) % 1.0
+        self.k += 1
+        r0 = min(self.ndets - rows, int(frac * (self.ndets - rows + 1)))
+        d = ctypes.c_double()
+        t = self.L.ref_sigma_step_timed(r0, rows, ctypes.byref(d))
+        return t, rows
+
+    def close(self):
+        self.L.ref_sigma_release()
+
+
+def calibrate(rs, small, large):
+    """The reference's fixed cost per call (buffer setup, whole-vector gets
+    and reductions) and its cost per row, from one block of each size."""
+    t1, r1 = rs.step(small)
+    t2, r2 = rs.step(large)
+    per_row = max((t2 - t1) / max(r2 - r1, 1), 1e-12)
+    return max(t1 - per_row * r1, 0.0), per_row
 
 
 def run_reference(a):
     rank = env_int("RANK", 0)
     if rank != 0:
         return 0
+    from oracle.oracle import ref_available
+    if not ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference build absent"}))
+        return 0
     (geo, nroots, s, d) = WORKLOADS[a.workload]
-    threads = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    os.environ.setdefault("OMP_SCHEDULE", "dynamic,64")
+    import math
+
     from jayci_b200.synth import WORKLOADS as W
     w = W[a.workload]
-    ndets = 1
-    import math
     ndets = math.comb(w["n"], w["k"]) ** 2
-    vals = []
-    sample = ""
-    for i in range(a.warmup + a.steps):
-        full_s, sample = reference_sigma_sample(a.workload, nroots, frac=a.ref_step_frac)
-        if full_s is None:
-            print(json.dumps({"impl": "reference", "unavailable": sample}))
-            return 0
-        if i >= a.warmup:
-            vals.append(full_s)
-    t = statistics.mean(vals)
-    value = ndets * nroots / t / 1e9
+    threads = host_threads(ndets, nroots)
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    os.environ.setdefault("OMP_SCHEDULE", "dynamic,64")
+    rs = RefSigma(a.workload, nroots)
+    # warm-up steps: the first two calibrate the fixed cost and the per-row
+    # cost; every timed step then runs the block that fits its time share
+    fixed, per_row = calibrate(rs, 2000, 20000)
+    for _ in range(max(0, a.warmup - 2)):
+        rs.step(2000)
+    budget = a.ref_seconds / max(a.steps, 1)
+    rows = int(max(2000, min(rs.ndets, (budget - fixed) / per_row)))
+    times, done = [], 0
+    for _ in range(a.steps):
+        t, r = rs.step(rows)
+        times.append(t)
+        done += r
+    rs.close()
+    tot = sum(times)
+    value = done * nroots / tot / 1e9
+    sample = (f"{a.steps} blocks of {rows} contiguous rows ({rows / ndets:.4%} of the "
+              f"determinants each), at rotating positions")
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Gdet/s",
            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-           "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+           "ms_per_step": tot / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded integrals)",
            "config": {"workload": a.workload, "ndets": ndets, "vectors_per_step": nroots,
+                      "rows_per_step": rows, "row_fraction_per_step": rows / ndets,
                       "sample": sample},
+           "reference_cost_model": {
+               "fixed_s_per_call": fixed, "s_per_row": per_row,
+               "extrapolated_full_sigma_s": fixed + per_row * ndets,
+               "note": "fixed cost and per-row cost from two calibration blocks "
+                       "(2000 and 20000 rows); the full-sigma time is an extrapolation"},
            "cpu_baseline": {"value": value, "unit": "Gdet/s", "cores": threads,
                             "kind": "reference", "sample": sample},
            "e2e": {"value": value, "unit": "Gdet/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
     return 0
+
+
+def cpu_baseline(name, nvec, seconds):
+    """The reference's sigma on one row block of about `seconds` of host
+    work (after two calibration blocks), as Gdet/s of the rows it ran."""
+    from oracle.oracle import ref_available
+    if not ref_available():
+        return None
+    import math
+
+    from jayci_b200.synth import WORKLOADS as W
+    w = W[name]
+    ndets = math.comb(w["n"], w["k"]) ** 2
+    threads = host_threads(ndets, nvec)
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    rs = RefSigma(name, nvec)
+    fixed, per_row = calibrate(rs, 2000, 20000)
+    rows = int(max(2000, min(rs.ndets, (seconds - fixed) / per_row)))
+    t, rows = rs.step(rows)
+    rs.close()
+    return {"value": rows * nvec / t / 1e9, "unit": "Gdet/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"reference sigma (diagonal term + compute_cblock_Hfastest), {nvec} "
+                      f"vector(s), one block of {rows} contiguous rows "
+                      f"({rows / ndets:.4%} of the determinants) in {t:.1f} s, "
+                      f"OMP_SCHEDULE={os.environ.get('OMP_SCHEDULE')}",
+            "fixed_s_per_call": fixed, "extrapolated_full_sigma_s": fixed + per_row * ndets}
+
+
+# ---- the GPU arm -----------------------------------------------------------
+
+def solve_pair(jb, name, world):
+    """The plain FP64 reference schedule against the mixed FP32 -> FP64
+    schedule on workload `name`, each timed after an untimed warm-up solve
+    of a few iterations (autotuning, graph capture, buffer allocation)."""
+    import numpy as np
+
+    from jayci_b200.synth import workload_integrals
+    (geo, nroots, _, _) = WORKLOADS[name]
+    ints = workload_integrals(name)
+    m1, m2 = ints.packed()
+    t0 = time.perf_counter()
+    sp = jb.Space(*geo)
+    sp.set_integrals(m1, m2, ints.e_nuc, ints.e_fc)
+    setup = time.perf_counter() - t0
+    kmin, kmax, refdim, maxiter = DALGINFO[name]
+    kw = dict(krymin=kmin, krymax=kmax, nroots=nroots, refdim=refdim, restol=1e-8)
+    first = {}
+    for p, key in ((jb.FP64, "fp64"), (jb.MIXED, "mixed")):
+        t0 = time.perf_counter()
+        sp.davidson(maxiter=kmax - kmin + 2, precision=p, want_vectors=False, **kw)
+        first[key] = time.perf_counter() - t0
+    r64 = sp.davidson(maxiter=maxiter, **kw)
+    rmx = sp.davidson(maxiter=maxiter, precision=jb.MIXED, **kw)
+    out = {"workload": name, "ndets": sp.ndets, "nroots": nroots,
+           "davidson": dict(krymin=kmin, krymax=kmax, refdim=refdim, maxiter=maxiter,
+                            restol=1e-8),
+           "fp64_solve_s": r64.stats.total_seconds, "fp64_converged": r64.converged,
+           "mixed_solve_s": rmx.stats.total_seconds, "mixed_converged": rmx.converged,
+           "fp64_sigma_vectors": r64.stats.sigma_vectors,
+           "mixed_sigma_vectors": {"fp32": rmx.stats.fp32_sigma_vectors,
+                                   "fp64": rmx.stats.sigma_vectors -
+                                   rmx.stats.fp32_sigma_vectors},
+           "fp64_sigma_s": r64.stats.sigma_seconds, "mixed_sigma_s": rmx.stats.sigma_seconds,
+           "fp64_solves_per_s": world / r64.stats.total_seconds,
+           "mixed_solves_per_s": world / rmx.stats.total_seconds,
+           "mixed_vs_fp64_max_abs_dE": float(np.abs(rmx.energies - r64.energies).max()),
+           "energies_fp64": [float(x) for x in r64.energies],
+           "mixed_speedup": r64.stats.total_seconds / rmx.stats.total_seconds,
+           "sigma_plans": {"fp64": sigma_plan_desc(*sp.sigma_tuning(jb.FP64)[:4]),
+                           "fp32": sigma_plan_desc(*sp.sigma_tuning(jb.FP32)[:4])},
+           "first_call_s": {"space_and_tables": setup,
+                            "warmup_solve_fp64": first["fp64"],
+                            "warmup_solve_mixed": first["mixed"]}}
+    sp.close()
+    return out
 
 
 def run_gpu(a):
@@ -282,8 +418,14 @@ def run_gpu(a):
     (geo, nroots, s_exc, d_exc) = WORKLOADS[a.workload]
     ints = workload_integrals(a.workload)
     m1, m2 = ints.packed()
+    setup = {}
+    t0 = time.perf_counter()
     sp = jb.Space(*geo)
+    setup["space_tables_host_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
     sp.set_integrals(m1, m2, ints.e_nuc, ints.e_fc)
+    torch.cuda.synchronize()
+    setup["set_integrals_s"] = time.perf_counter() - t0
     N, nvec = sp.ndets, nroots
     stream = torch.cuda.Stream()
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
@@ -314,6 +456,14 @@ def run_gpu(a):
         launches = [e[0].elapsed_time(e[1]) for row in ev for e in row]
         return sum(launches), launches
 
+    # first sigma call of each precision: the autotuner times the plans
+    for prec, v, o, key in ((jb.FP64, V, S, "autotune_fp64_s"), (jb.FP32, V32, S32,
+                                                                  "autotune_fp32_s")):
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            sp.sigma_device(v[0].data_ptr(), o[0].data_ptr(), 1, N, prec, sh)
+        torch.cuda.synchronize()
+        setup[key] = time.perf_counter() - t0
     with torch.cuda.stream(stream):
         for _ in range(a.warmup):
             step(None)
@@ -333,6 +483,7 @@ def run_gpu(a):
     tot_ms, tot32_ms = max_over_ranks(dist, [tot_ms, tot32_ms], "cuda")
     value = replica_rate(world, N * nvec * a.steps, tot_ms / 1e3) / 1e9
     value32 = replica_rate(world, N * nvec * a.steps, tot32_ms / 1e3) / 1e9
+    del V32, S32
 
     # end to end through the C ABI from pinned host memory
     hv = torch.randn(nvec, N, dtype=torch.float64, generator=torch.Generator().manual_seed(7))
@@ -344,17 +495,18 @@ def run_gpu(a):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    e2e_s = 0.0
     for _ in range(a.steps):
         flush.fill_(1.0)
         torch.cuda.synchronize()
+        t0 = time.perf_counter()
         rc = jb.lib().jci_sigma(sp.h, nvec, hvn.ctypes.data, hsn.ctypes.data, jb.FP64)
+        e2e_s += time.perf_counter() - t0
         if rc:
             raise jb.JciError(rc, "jci_sigma")
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
     e2e_s, = max_over_ranks(dist, [e2e_s], "cuda")
     e2e = replica_rate(world, N * nvec * a.steps, e2e_s) / 1e9
+    del hv, hs, hvn, hsn
 
     # roofline of the sigma kernel (row-stream algorithmic bytes per vector)
     w = 8
@@ -362,55 +514,46 @@ def run_gpu(a):
     avg_launch_s = statistics.mean(launches) / 1e3
     peak, peak_kind = measured_peaks()
     achieved = bytes_per_launch / avg_launch_s / 1e9
-    mode, nt, R, B, _ = sp.sigma_tuning(jb.FP64)
-    traffic = committed_traffic(a.workload, mode, B)
+    mode, nt, R, B, tms = sp.sigma_tuning(jb.FP64)
+    tune32 = sp.sigma_tuning(jb.FP32)
+    prof = committed_profile(a.workload, mode, B) or {}
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic,
+            "frac": achieved / peak, "traffic": prof.get("dram_bytes_per_launch"),
             "algorithmic_bytes_per_launch": bytes_per_launch, "peak_source": peak_kind,
-            "kernel_ms_per_launch": avg_launch_s * 1e3}
+            "kernel_ms_per_launch": avg_launch_s * 1e3,
+            "model": "row-stream bytes B = 8 N (2 + s + d) per vector: each sigma row reads "
+                     "its own C row and one C row per alpha single and double"}
+    for k in ("dram_gb_per_s", "l2_bytes_per_launch", "limiter", "summary"):
+        if k in prof:
+            roof[k] = prof[k]
+    sp.close()
+    del V, S
+    torch.cuda.empty_cache()
 
-    # full solves (outside the timed region): reference schedule FP64 vs mixed block
     solves = {}
     if not a.no_solves:
-        kmin, kmax, refdim, maxiter = DALGINFO[a.workload]
-        kw = dict(maxiter=maxiter, krymin=kmin, krymax=kmax, nroots=nroots, refdim=refdim,
-                  restol=1e-8)
-        r64 = sp.davidson(**kw)
-        rmx = sp.davidson(precision=jb.MIXED, **kw)
-        solves = {"fp64_solve_s": r64.stats.total_seconds, "fp64_converged": r64.converged,
-                  "mixed_solve_s": rmx.stats.total_seconds, "mixed_converged": rmx.converged,
-                  "fp64_sigma_vectors": r64.stats.sigma_vectors,
-                  "mixed_sigma_vectors": [rmx.stats.fp32_sigma_vectors,
-                                          rmx.stats.sigma_vectors - rmx.stats.fp32_sigma_vectors],
-                  "davidson": dict(krymin=kmin, krymax=kmax, refdim=refdim, maxiter=maxiter),
-                  "fp64_solves_per_s": world / r64.stats.total_seconds,
-                  "mixed_solves_per_s": world / rmx.stats.total_seconds,
-                  "mixed_vs_fp64_max_abs_dE": float(np.abs(rmx.energies - r64.energies).max()),
-                  "energies_fp64": [float(x) for x in r64.energies],
-                  "mixed_speedup": r64.stats.total_seconds / rmx.stats.total_seconds}
+        solves = solve_pair(jb, SOLVES_OF[a.workload], world)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        full_s, sample = reference_sigma_sample(a.workload, nvec, frac=a.ref_frac)
-        if full_s is not None:
-            cpu = {"value": N * nvec / full_s / 1e9, "unit": "Gdet/s",
-                   "cores": os.cpu_count(), "kind": "reference",
-                   "sample": f"reference sigma (compute_cblock_Hfastest), {nvec} vectors, "
-                             f"{sample}, OMP_SCHEDULE=dynamic,64"}
+        cpu = cpu_baseline(a.workload, nvec, a.cpu_seconds)
     out = {"metric": METRIC, "value": value, "unit": "Gdet/s", "n_gpus": world,
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": tot_ms / a.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded integrals, random CI vectors)",
            "config": {"workload": a.workload, "ndets": N, "vectors_per_step": nvec,
                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                      "l2": "flushed (256 MiB write) before every step",
-                      "sigma_plan": sigma_plan_desc(mode, nt, R, B)},
+                      "l2": "inputs (8 bytes x ndets per vector) larger than L2; a 256 MiB "
+                            "write also flushes it before every step",
+                      "sigma_plan": sigma_plan_desc(mode, nt, R, B, tms),
+                      "sigma_plan_fp32": sigma_plan_desc(*tune32)},
            "roofline": roof, "cpu_baseline": cpu,
            "e2e": {"value": e2e, "unit": "Gdet/s", "h2d_bytes_per_step": nvec * N * 8,
                    "d2h_bytes_per_step": nvec * N * 8},
            "gpu_launches": a.steps * nvec * SIGMA_KERNELS[mode],
            "clocks": clk,
            "fp32_sigma_gdet_s": value32,
+           "setup_s": setup,
            "solves": solves}
     tp = committed_tensor_pipe(a.workload)
     if tp:
@@ -625,21 +768,20 @@ def run_profile(a):
 
 def main():
     # the reference's sigma kernel runs its OpenMP loop with schedule(runtime):
-    # every CPU timing here uses all host threads and the same schedule
-    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    # every CPU timing here uses the same schedule
     os.environ.setdefault("OMP_SCHEDULE", "dynamic,64")
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="jci", choices=["jci", "reference"])
-    ap.add_argument("--workload", default="fci12_12", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="fci16_16", choices=sorted(WORKLOADS))
     ap.add_argument("--no-solves", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--ref-frac", type=float, default=0.25,
-                    help="fraction of rows in the CPU-baseline sample (about 10 s)")
-    ap.add_argument("--ref-step-frac", type=float, default=0.25,
-                    help="fraction of rows per step of --impl reference")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="host seconds of the CPU-baseline sample")
+    ap.add_argument("--ref-seconds", type=float, default=120.0,
+                    help="host seconds of all timed steps of --impl reference together")
     ap.add_argument("--serve", type=int, default=0,
                     help="run the serving stream with this many requests instead")
     ap.add_argument("--slots", type=int, default=8)

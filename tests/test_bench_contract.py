@@ -7,17 +7,22 @@ import os
 import bench
 
 
+def _traffic(workload, mode, B):
+    p = bench.committed_profile(workload, mode, B)
+    return p.get("dram_bytes_per_launch") if p else None
+
+
 def test_traffic_is_looked_up_per_plan_and_group_variant():
     # FCI(12,12): plan 5 and plan 7 with group variants 2 and 3 were captured
-    assert bench.committed_traffic("fci12_12", 5, 1) > 0
-    assert bench.committed_traffic("fci12_12", 7, 3) > 0
-    assert bench.committed_traffic("fci12_12", 7, 2) > 0
+    assert _traffic("fci12_12", 5, 1) > 0
+    assert _traffic("fci12_12", 7, 3) > 0
+    assert _traffic("fci12_12", 7, 2) > 0
     # plans or variants without a capture report no traffic
-    assert bench.committed_traffic("fci12_12", 7, 4) is None
-    assert bench.committed_traffic("fci12_12", 1, 1) is None
-    assert bench.committed_traffic("fci14_14_fc2", 6, 2) > 0
-    assert bench.committed_traffic("fci14_14_fc2", 6, 3) is None
-    assert bench.committed_traffic("no_such_workload", 5, 1) is None
+    assert _traffic("fci12_12", 7, 4) is None
+    assert _traffic("fci12_12", 1, 1) is None
+    assert _traffic("fci14_14_fc2", 6, 2) > 0
+    assert _traffic("fci14_14_fc2", 6, 3) is None
+    assert _traffic("no_such_workload", 5, 1) is None
 
 
 def test_every_traffic_entry_points_at_a_committed_summary():
@@ -57,3 +62,44 @@ def test_tensor_pipe_figures_come_from_committed_captures():
         assert 0 < k["active_pct"] <= 100
         assert os.path.exists(os.path.join(bench.ROOT, k["summary"]))
     assert bench.committed_tensor_pipe("cas10_10") is None
+
+
+def test_default_workload_is_the_largest_single_gpu_configuration():
+    import sys
+    old = sys.argv
+    try:
+        sys.argv = ["bench.py"]
+        import argparse
+        seen = {}
+        real = argparse.ArgumentParser.parse_args
+
+        def grab(self, *a, **k):
+            ns = real(self, *a, **k)
+            seen["ns"] = ns
+            raise SystemExit(0)
+        argparse.ArgumentParser.parse_args = grab
+        try:
+            bench.main()
+        except SystemExit:
+            pass
+        finally:
+            argparse.ArgumentParser.parse_args = real
+    finally:
+        sys.argv = old
+    assert seen["ns"].workload == "fci16_16"
+    assert bench.SOLVES_OF["fci16_16"] == "fci14_14_fc2"
+
+
+def test_reference_calibration_separates_fixed_and_row_costs():
+    class Fake:
+        """A reference whose call costs 4 s plus 1 ms per row."""
+        def step(self, rows):
+            return 4.0 + 1e-3 * rows, rows
+    fixed, per_row = bench.calibrate(Fake(), 2000, 20000)
+    assert abs(fixed - 4.0) < 1e-9 and abs(per_row - 1e-3) < 1e-12
+
+
+def test_reference_threads_are_bounded_by_memory():
+    # one full-length private buffer per thread: a huge vector gets one thread
+    assert bench.host_threads(10 ** 13, 1) == 1
+    assert 1 <= bench.host_threads(1000, 1) <= (os.cpu_count() or 1)
