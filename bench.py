@@ -200,11 +200,15 @@ class ClockSampler:
 # ---- the reference's own sigma on the host cores ---------------------------
 
 def host_threads(ndets, nvec):
-    """Host threads for the reference's sigma: every core, bounded by memory.
-    compute_hij_eosp keeps a private full-length sigma buffer per OpenMP
-    thread (pdavidson.c:1930-2078), nvec x ndets doubles each, beside
-    about 5 x that of shared arrays (V, C, D, W and the row buffers)."""
-    cores = os.cpu_count() or 1
+    """Host threads for the reference's sigma: every core, bounded by memory
+    and by the reference's own size arithmetic.  compute_hij_eosp keeps a
+    private full-length sigma buffer per OpenMP thread (pdavidson.c:1930-2078),
+    nvec x ndets doubles each, beside about 5 x that of shared arrays (V, C,
+    D, W and the row buffers).  It allocates them as one block whose element
+    count nvec x ndets x threads is an int (pdavidson.c:1946, allocate_mem.c:58):
+    past 2^31 - 1 the product wraps, the allocation fails and the reference
+    crashes, so FCI(16e,16o) runs on at most 12 threads."""
+    cores = min(os.cpu_count() or 1, max(1, (2 ** 31 - 1) // max(1, nvec * ndets)))
     try:
         import psutil
         avail = psutil.virtual_memory().available

@@ -10,6 +10,8 @@ imports this module.
   mpi_source C code compiled unchanged against a single-process GA/MPI
   stand-in (only present where the reference tree was available at build
   time; see Makefile).
+* :func:`ref_serial_solve` wraps ``_ref/libjayci_serial.so`` -- the
+  reference's serial source/ path (the jayci program) compiled unchanged.
 """
 from __future__ import annotations
 
@@ -23,6 +25,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libjayci_ref.so")
+SERIAL_SO = os.path.join(HERE, "_ref", "libjayci_serial.so")
 
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 
@@ -60,6 +63,53 @@ def _load(path):
 
 def ref_available() -> bool:
     return os.path.exists(REF_SO)
+
+
+def serial_available() -> bool:
+    return os.path.exists(SERIAL_SO)
+
+
+_serial = None
+
+
+def ref_serial_solve(general, m1, m2, nucrep, frzcore=0.0, maxiter=500, krymin=4,
+                     krymax=12, nroots=1, prediagr=1, refdim=8, restol=1e-8, printlvl=0,
+                     want_vectors=True):
+    """The reference's serial jayci path (oracle/_ref/libjayci_serial.so,
+    source/*.c compiled unchanged): citrunc_rtnlist, the O(N^2) cimap,
+    compute_hdgls and dvdalg.  general = (electrons, orbitals, nfrozen,
+    ndocc, nactive, nfrzvirt, xlevel).  Returns (energies including
+    nucrep + frzcore, civec nroots x ndets or None, times {cimap, hdgls,
+    dvdalg} in seconds)."""
+    global _serial
+    if _serial is None:
+        if not os.path.exists(SERIAL_SO):
+            raise FileNotFoundError(SERIAL_SO)
+        L = ctypes.CDLL(SERIAL_SO)
+        L.ref_serial_solve.restype = ctypes.c_longlong
+        L.ref_serial_solve.argtypes = [ctypes.c_int] * 7 + [ctypes.c_void_p] * 2 + \
+            [ctypes.c_double] * 2 + [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_int] + \
+            [ctypes.c_void_p] * 3
+        _serial = L
+    e, o, nfc, nd, na, nfv, x = (int(v) for v in general)
+    ci_e = e - 2 * nfc
+    sp = OracleSpace((ci_e + 1) // 2, ci_e // 2, o - nfc - nfv, nd, na, x)
+    n = sp.ndets
+    del sp
+    m1 = np.ascontiguousarray(m1, float)
+    m2 = np.ascontiguousarray(m2, float)
+    en = np.zeros(nroots)
+    civ = np.zeros((nroots, n)) if want_vectors else None
+    times = np.zeros(3)
+    r = _serial.ref_serial_solve(e, o, nfc, nd, na, nfv, x, _ptr(m1), _ptr(m2), nucrep,
+                                 frzcore, maxiter, krymin, krymax, nroots, prediagr, refdim,
+                                 restol, printlvl, _ptr(en),
+                                 _ptr(civ) if civ is not None else None, _ptr(times))
+    if r < 0:
+        raise RuntimeError(f"reference serial solve failed ({r})")
+    if r != n:
+        raise RuntimeError(f"reference serial space has {r} determinants, expected {n}")
+    return en, civ, dict(cimap=times[0], hdgls=times[1], dvdalg=times[2])
 
 
 class OracleSpace:

@@ -103,3 +103,5 @@ def test_reference_threads_are_bounded_by_memory():
     # one full-length private buffer per thread: a huge vector gets one thread
     assert bench.host_threads(10 ** 13, 1) == 1
     assert 1 <= bench.host_threads(1000, 1) <= (os.cpu_count() or 1)
+    # the reference's int-sized buffer block: FCI(16e,16o) fits 12 threads
+    assert bench.host_threads(165636900, 1) <= 12

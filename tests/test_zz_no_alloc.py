@@ -6,9 +6,10 @@ device-memory budget, an application whose allocator forbids device
 allocation after start-up.  For them libjci offers a sigma whose scratch
 panels live in a fixed 64 MiB device array inside the library.  This file
 checks it through the C ABI against the ordinary entry point
-(jci_sigma_device) on two consecutive calls, with the same tolerances as the
-other sigma tests (FP64 1e-12, FP32 2e-6 of max|sigma|), and checks that the
-device's free memory does not move across its first call on a fresh space.
+(jci_sigma_device) on two consecutive calls, with the tolerances of the
+other sigma tests (FP64 1e-12, FP32 2e-6 of max|sigma| from the exact sigma,
+so two FP32 results agree within 4e-6), and checks that the device's free
+memory does not move across its first call on a fresh space.
 It is named so that pytest collects it last.
 """
 import ctypes
@@ -59,9 +60,13 @@ def _vector(n, prec, seed):
 
 
 def _check_two_calls(s, v, ref, prec, stream):
-    """Two noalloc calls in a row into NaN-filled outputs, each against ref."""
+    """Two noalloc calls in a row into NaN-filled outputs, each against ref,
+    the existing entry point's output in the same precision.  The two may
+    sum in different orders (the entry point runs its tuned plan): in FP64
+    they agree to 1e-12; in FP32 each lies within 2e-6 of the exact sigma,
+    so they agree within twice that."""
     import torch
-    tol = TOL[prec] * ref.abs().max().item()
+    tol = (1 if prec == jb.FP64 else 2) * TOL[prec] * ref.abs().max().item()
     out = None
     for _ in range(2):  # consecutive calls share the static scratch array
         out = torch.full_like(v, float("nan"))
@@ -122,7 +127,7 @@ def test_noalloc_first_call_allocates_nothing(n, prec):
     ref = torch.empty_like(v)
     s.sigma_device(v.data_ptr(), ref.data_ptr(), 1, s.ndets, prec, 0)
     torch.cuda.synchronize()
-    tol = TOL[prec] * ref.abs().max().item()
+    tol = (1 if prec == jb.FP64 else 2) * TOL[prec] * ref.abs().max().item()
     assert (out - ref).abs().max().item() <= tol
     _check_two_calls(s, v, ref, prec, 0)
     s.close()
@@ -139,11 +144,17 @@ PLANS = [(0, 128, 2, 1), (0, 512, 4, 1), (1, 128, 0, 1), (1, 1024, 0, 1), (2, 25
 @pytest.mark.parametrize("prec", [jb.FP64, jb.FP32])
 def test_noalloc_after_every_forced_plan(prec):
     """FCI(14e,14o): every admissible forced plan, then noalloc against
-    jci_sigma_device under that plan."""
+    jci_sigma_device under that plan; in FP32 also against the FP64 sigma
+    of the same vector at the FP32 bar."""
     import torch
     s = _cas(14, 3)
     v = _vector(s.ndets, prec, 9)
     ref = torch.empty_like(v)
+    v64 = v.double()
+    exact = torch.empty_like(v64)
+    s.sigma_device(v64.data_ptr(), exact.data_ptr(), 1, s.ndets, jb.FP64, 0)
+    torch.cuda.synchronize()
+    bar = TOL[prec] * exact.abs().max().item()
     ran = 0
     for mode, nt, rows, batch in PLANS:
         try:
@@ -154,7 +165,8 @@ def test_noalloc_after_every_forced_plan(prec):
         ref.fill_(float("nan"))
         s.sigma_device(v.data_ptr(), ref.data_ptr(), 1, s.ndets, prec, 0)
         torch.cuda.synchronize()
-        _check_two_calls(s, v, ref, prec, 0)
+        out = _check_two_calls(s, v, ref, prec, 0)
+        assert (out.double() - exact).abs().max().item() <= bar
         ran += 1
     assert ran >= 10
     s.close()
