@@ -370,16 +370,35 @@ jci_status jci_read_namelists(const char *path, jci_general *g,
 /* Read a SIFS integral file (readmoints.f90:21 with colib sifrsh/sifd2):
  * moints1 (m1cap doubles) and moints2 (m2cap doubles) are zeroed and
  * filled in index1e/index2e packing; *nbft receives the orbital count,
- * *nucrep energy(1) of header 2, *frzcore the H1 core energy. */
+ * *nucrep energy(1) of header 2, *frzcore the H1 core energy.  fsplit 1
+ * and 2 (below) are both read. */
 jci_status jci_read_moints(const char *path, double *moints1, long long m1cap,
                            double *moints2, long long m2cap, int *nbft,
                            double *nucrep, double *frzcore);
+
+/* Files with fsplit = 2 (info(1) of header 2) keep their 2-e records on a
+ * second file, opened by colib's sifo2f (colib8.f:1720) as a plain
+ * sequential file of l2rec-word records; the reference's reader refuses
+ * them (readmoints.f90:278-282).  jci_read_moints takes them with the 2-e
+ * file named path + "2" (moints / moints2, as colib's callers pair
+ * aoints / aoints2); jci_read_moints_split names the 2-e file itself (it
+ * is only opened when the header says fsplit = 2). */
+jci_status jci_read_moints_split(const char *path, const char *path2,
+                                 double *moints1, long long m1cap,
+                                 double *moints2, long long m2cap, int *nbft,
+                                 double *nucrep, double *frzcore);
 
 /* Write a single-symmetry SIFS file with the given packed integrals
  * (colib sifwh / sifew1 / sifew2 layout, 8-bit labels, fsplit = 1). */
 jci_status jci_write_moints(const char *path, int nbft,
                             const double *moints1, const double *moints2,
                             double nucrep, double frzcore);
+/* The same with fsplit = 2: headers and 1-e records on path, the 2-e
+ * records on path2 (sifew2 through colib's aiwrit, colib2.f:178). */
+jci_status jci_write_moints_split(const char *path, const char *path2,
+                                  int nbft, const double *moints1,
+                                  const double *moints2, double nucrep,
+                                  double frzcore);
 
 /* Unformatted vector files "civec" / "ci.restart" / "hvvec":
  * int32 dim, int32 len, dim*len float64 (mpi_utilities.c:353,430). */

@@ -378,24 +378,41 @@ def sifs_nbft(path):
     return int(np.frombuffer(head[4:60], np.int64)[3])
 
 
-def read_moints(path):
-    """SIFS integrals -> (moints1, moints2, nbft, nucrep, frzcore)."""
+def read_moints(path, path2=None):
+    """SIFS integrals -> (moints1, moints2, nbft, nucrep, frzcore).  Files
+    with fsplit = 2 take their 2-e records from path2 (default: path + "2")."""
     m1len, m2len = moint_sizes(sifs_nbft(path))
     m1 = np.zeros(m1len)
     m2 = np.zeros(m2len)
     nb, en, fc = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
-    _check(lib().jci_read_moints(str(path).encode(), _p(m1), m1len, _p(m2), m2len,
-                                 ctypes.byref(nb), ctypes.byref(en), ctypes.byref(fc)),
-           "read_moints")
+    if path2 is None:
+        st = lib().jci_read_moints(str(path).encode(), _p(m1), m1len, _p(m2), m2len,
+                                   ctypes.byref(nb), ctypes.byref(en), ctypes.byref(fc))
+    else:
+        f = lib().jci_read_moints_split
+        f.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_longlong,
+                      ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int),
+                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        st = f(str(path).encode(), str(path2).encode(), _p(m1), m1len, _p(m2), m2len,
+               ctypes.byref(nb), ctypes.byref(en), ctypes.byref(fc))
+    _check(st, "read_moints")
     a, b = moint_sizes(nb.value)
     return m1[:a].copy(), m2[:b].copy(), nb.value, en.value, fc.value
 
 
-def write_moints(path, nbft, moints1, moints2, nucrep, frzcore=0.0):
+def write_moints(path, nbft, moints1, moints2, nucrep, frzcore=0.0, path2=None):
+    """Write SIFS integrals; with path2 the file has fsplit = 2 and its 2-e
+    records go to path2."""
     m1 = np.ascontiguousarray(moints1, np.float64)
     m2 = np.ascontiguousarray(moints2, np.float64)
-    _check(lib().jci_write_moints(str(path).encode(), nbft, _p(m1), _p(m2), nucrep, frzcore),
-           "write_moints")
+    if path2 is None:
+        st = lib().jci_write_moints(str(path).encode(), nbft, _p(m1), _p(m2), nucrep, frzcore)
+    else:
+        f = lib().jci_write_moints_split
+        f.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p,
+                      ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        st = f(str(path).encode(), str(path2).encode(), nbft, _p(m1), _p(m2), nucrep, frzcore)
+    _check(st, "write_moints")
 
 
 def write_vectors(path, v):

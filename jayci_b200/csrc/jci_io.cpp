@@ -241,9 +241,29 @@ long long ix1(long long i, long long j) {
 
 }  // namespace
 
-extern "C" jci_status jci_read_moints(const char *path, double *m1, long long m1cap, double *m2,
-                                      long long m2cap, int *nbft_out, double *nucrep,
-                                      double *frzcore) {
+// 2-e records (sifd2 with nipv = 4, colib8.f:447) from r into m2, until the
+// record flagged last = 2.
+static bool read_2e_records(Reader &r, long long l2rec, long long nbft, double *m2) {
+    int last = 0;
+    do {
+        if (!r.next() || (long long)r.words() < l2rec) return false;
+        Dword dw = unpack_dword((uint64_t)r.i64(0));
+        last = dw.last;
+        if (dw.ifmt != 0 || 1 + dw.num > (long long)r.words()) return false;
+        for (int k = 0; k < dw.num; k++) {
+            int l[4];
+            for (int q = 0; q < 4; q++) l[q] = label8(r, dw.lab1 - 1, 4LL * k + q);
+            for (int q = 0; q < 4; q++)
+                if (l[q] < 1 || l[q] > nbft) return false;
+            m2[ix1(ix1(l[0], l[1]), ix1(l[2], l[3])) - 1] += r.f64(1 + k);
+        }
+    } while (last != 2);
+    return true;
+}
+
+static jci_status read_moints(const char *path, const char *path2, double *m1, long long m1cap,
+                              double *m2, long long m2cap, int *nbft_out, double *nucrep,
+                              double *frzcore) {
     if (!path || !m1 || !m2) return JCI_ERR_ARG;
     FILE *f = fopen(path, "rb");
     if (!f) return JCI_ERR_IO;
@@ -272,7 +292,10 @@ extern "C" jci_status jci_read_moints(const char *path, double *m1, long long m1
         double e1;
         memcpy(&e1, &r.rec[off], 8);  // energy(1)
         long long l1rec = info[1], n1max = info[2], l2rec = info[3];
-        if (info[0] != 1) break;  // fsplit = 2: separate 2-e file (readmoints.f90:278)
+        // fsplit (info(1)): 1 = the 2-e records follow on this file; 2 = they
+        // are on a second file (colib sifo2f, colib8.f:1720), which the
+        // reference refuses (readmoints.f90:278-282) and this reader takes
+        if (info[0] != 1 && info[0] != 2) break;
         if (info[5] != 0) break;  // only 8-bit label packing
         memset(m1, 0, sizeof(double) * m1cap);
         memset(m2, 0, sizeof(double) * m2cap);
@@ -305,29 +328,23 @@ extern "C" jci_status jci_read_moints(const char *path, double *m1, long long m1
             }
         } while (ok && last != 2);
         if (!ok) break;
-        // 2-e records (sifd2, nipv = 4)
-        last = 0;
-        do {
-            if (!r.next() || (long long)r.words() < l2rec) {
-                ok = false;
+        if (info[0] == 1) {
+            if (!read_2e_records(r, l2rec, nbft, m2)) break;
+        } else {
+            // the second file holds only the 2-e records, one sequential
+            // unformatted record of l2rec words each (colib aiopen/airead,
+            // colib2.f:34,89)
+            std::string p2 = path2 ? std::string(path2) : std::string(path) + "2";
+            FILE *f2 = fopen(p2.c_str(), "rb");
+            if (!f2) {
+                st = JCI_ERR_IO;
                 break;
             }
-            Dword dw = unpack_dword((uint64_t)r.i64(0));
-            last = dw.last;
-            if (dw.ifmt != 0 || 1 + dw.num > (long long)r.words()) {
-                ok = false;
-                break;
-            }
-            for (int k = 0; k < dw.num; k++) {
-                int l[4];
-                for (int q = 0; q < 4; q++) l[q] = label8(r, dw.lab1 - 1, 4LL * k + q);
-                for (int q = 0; q < 4; q++)
-                    if (l[q] < 1 || l[q] > nbft) ok = false;
-                if (!ok) break;
-                m2[ix1(ix1(l[0], l[1]), ix1(l[2], l[3])) - 1] += r.f64(1 + k);
-            }
-        } while (ok && last != 2);
-        if (!ok) break;
+            Reader r2{f2, {}};
+            ok = read_2e_records(r2, l2rec, nbft, m2);
+            fclose(f2);
+            if (!ok) break;
+        }
         if (nbft_out) *nbft_out = (int)nbft;
         if (nucrep) *nucrep = e1;
         if (frzcore) *frzcore = hcore;
@@ -335,6 +352,19 @@ extern "C" jci_status jci_read_moints(const char *path, double *m1, long long m1
     } while (0);
     fclose(f);
     return st;
+}
+
+extern "C" jci_status jci_read_moints(const char *path, double *m1, long long m1cap, double *m2,
+                                      long long m2cap, int *nbft_out, double *nucrep,
+                                      double *frzcore) {
+    return read_moints(path, nullptr, m1, m1cap, m2, m2cap, nbft_out, nucrep, frzcore);
+}
+
+extern "C" jci_status jci_read_moints_split(const char *path, const char *path2, double *m1,
+                                            long long m1cap, double *m2, long long m2cap,
+                                            int *nbft_out, double *nucrep, double *frzcore) {
+    if (!path2) return JCI_ERR_ARG;
+    return read_moints(path, path2, m1, m1cap, m2, m2cap, nbft_out, nucrep, frzcore);
 }
 
 namespace {
@@ -354,12 +384,19 @@ void put_label8(std::vector<uint64_t> &buf, size_t w0, long long k, int v) {
 
 }  // namespace
 
-extern "C" jci_status jci_write_moints(const char *path, int nbft, const double *m1,
-                                       const double *m2, double nucrep, double frzcore) {
+// fsplit 1 when path2 is null (every record on path), else 2 (the 2-e
+// records on path2, as colib's sifew2 writes them through aiwrit).
+static jci_status write_moints(const char *path, const char *path2, int nbft, const double *m1,
+                               const double *m2, double nucrep, double frzcore) {
     if (!path || !m1 || !m2 || nbft < 1 || nbft > 255) return JCI_ERR_ARG;
     const long long l1rec = 4096, n1max = 3272, l2rec = 4096, n2max = 2730;
     FILE *f = fopen(path, "wb");
     if (!f) return JCI_ERR_IO;
+    FILE *f2 = nullptr;
+    if (path2 && !(f2 = fopen(path2, "wb"))) {
+        fclose(f);
+        return JCI_ERR_IO;
+    }
     Writer w{f};
     bool ok = true;
     // header 1: version, ntitle, nsym, nbft, ninfo, nenrgy, nmap
@@ -377,7 +414,7 @@ extern "C" jci_status jci_write_moints(const char *path, int nbft, const double 
     int64_t nb = nbft;
     put(&nb, 8);
     put("a   ", 4);
-    int64_t info[6] = {1, l1rec, n1max, l2rec, n2max, 0};
+    int64_t info[6] = {f2 ? 2 : 1, l1rec, n1max, l2rec, n2max, 0};
     put(info, sizeof(info));
     for (int i = 1; i <= nbft; i++) {
         char lab[9];
@@ -432,6 +469,7 @@ extern "C" jci_status jci_write_moints(const char *path, int nbft, const double 
                     v2.push_back({(uint32_t)(i << 24 | j << 16 | k << 8 | l), v});
                 }
     if (v2.empty()) v2.push_back({(1u << 24) | (1u << 16) | (1u << 8) | 1u, 0.0});
+    Writer w2{f2 ? f2 : f};
     size_t pos = 0;
     while (pos < v2.size() && ok) {
         int num = (int)std::min<size_t>(n2max, v2.size() - pos);
@@ -445,11 +483,24 @@ extern "C" jci_status jci_write_moints(const char *path, int nbft, const double 
             for (int q = 0; q < 4; q++)
                 put_label8(buf, lab1 - 1, 4LL * k + q, (int)((lab >> (24 - 8 * q)) & 0xff));
         }
-        ok &= w.rec(buf.data(), buf.size() * 8);
+        ok &= w2.rec(buf.data(), buf.size() * 8);
         pos += num;
     }
+    if (f2) ok &= fclose(f2) == 0;
     ok &= fclose(f) == 0;
     return ok ? JCI_OK : JCI_ERR_IO;
+}
+
+extern "C" jci_status jci_write_moints(const char *path, int nbft, const double *m1,
+                                       const double *m2, double nucrep, double frzcore) {
+    return write_moints(path, nullptr, nbft, m1, m2, nucrep, frzcore);
+}
+
+extern "C" jci_status jci_write_moints_split(const char *path, const char *path2, int nbft,
+                                             const double *m1, const double *m2, double nucrep,
+                                             double frzcore) {
+    if (!path2) return JCI_ERR_ARG;
+    return write_moints(path, path2, nbft, m1, m2, nucrep, frzcore);
 }
 
 // ---- vector files --------------------------------------------------------

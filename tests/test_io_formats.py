@@ -41,6 +41,48 @@ def test_sifs_round_trip(tmp_path, nfrozen):
     np.testing.assert_allclose(eri, eri.transpose(2, 3, 0, 1))
 
 
+def test_sifs_fsplit2_separate_two_electron_file(tmp_path):
+    """fsplit = 2 (info(1) of header 2): the 2-e records sit on a second
+    file with no headers, one l2rec-word Fortran record each (colib sifo2f /
+    aiopen / airead, colib8.f:1720, colib2.f:34,89).  The reference's
+    readmoints.f90:278-282 refuses such files; this reader takes them."""
+    ints = make_integrals(7, 7, 23, nfrozen=1)
+    m1, m2 = ints.packed()
+    one = tmp_path / "one" / "moints"
+    one.parent.mkdir()
+    jb.write_moints(one, 7, m1, m2, ints.e_nuc, ints.e_fc)
+    p, p2 = tmp_path / "moints", tmp_path / "moints2"
+    jb.write_moints(p, 7, m1, m2, ints.e_nuc, ints.e_fc, path2=p2)
+    # header 2 says fsplit = 2; the 1-e file is shorter by the 2-e records
+    raw, raw2 = p.read_bytes(), p2.read_bytes()
+    n2 = struct.unpack("<i", raw[64:68])[0]  # header 2 follows the 64-byte header 1
+    off = 68 + 80 + 8 + 4                     # title, nbpsy, slabel
+    info = struct.unpack("<6q", raw[off:off + 48])
+    assert info[0] == 2 and info[3] == 4096
+    assert n2 > 0 and len(raw) + len(raw2) == len(one.read_bytes())
+    # the 2-e file starts with a 2-e record (itypea 3 in the dword)
+    assert struct.unpack("<i", raw2[:4])[0] == 8 * info[3]
+    dword = struct.unpack("<Q", raw2[4:12])[0]
+    assert ((dword >> 16) & 0xffff) >> 10 & 7 == 3
+    for got in (jb.read_moints(p), jb.read_moints(p, p2)):
+        r1, r2, nb, en, fc = got
+        assert (nb, en, fc) == (7, ints.e_nuc, ints.e_fc)
+        np.testing.assert_array_equal(r1, m1)
+        np.testing.assert_array_equal(r2, m2)
+    # a missing 2-e file is an I/O error, a truncated one a format error
+    p2.rename(tmp_path / "elsewhere")
+    with pytest.raises(jb.JciError) as e:
+        jb.read_moints(p)
+    assert e.value.status == 6
+    (tmp_path / "moints2").write_bytes(raw2[: len(raw2) // 2])
+    with pytest.raises(jb.JciError) as e:
+        jb.read_moints(p)
+    assert e.value.status == 7
+    # an fsplit = 1 file never opens the named 2-e file
+    r1, r2, *_ = jb.read_moints(one, tmp_path / "absent")
+    np.testing.assert_array_equal(r2, m2)
+
+
 def test_sifs_record_layout(tmp_path):
     """Header 1 is seven INTEGER*8 in one Fortran record (readmoints.f90:101);
     the first 1-e record's dword carries num/lab1/types/last as four 16-bit
