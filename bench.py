@@ -242,6 +242,10 @@ class RefSigma:
         self.ref = RefSpace(e, o, nfc)
         self.ndets, self.nvec = self.ref.ndets, nvec
         L = self.ref.lib()
+        # the thread count must reach the OpenMP runtime itself: it read
+        # OMP_NUM_THREADS when it started, possibly before this process set it
+        L.ref_set_threads(int(os.environ.get("OMP_NUM_THREADS", "0")))
+        self.threads = L.ref_get_threads()
         L.ref_sigma_step_timed.restype = ctypes.c_double
         L.ref_sigma_step_timed.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         V = np.random.default_rng(0).standard_normal((nvec, self.ndets))
@@ -304,6 +308,7 @@ def run_reference(a):
         times.append(t)
         done += r
     rs.close()
+    threads = rs.threads
     tot = sum(times)
     value = done * nroots / tot / 1e9
     sample = (f"{a.steps} blocks of {rows} contiguous rows ({rows / ndets:.4%} of the "
@@ -346,6 +351,7 @@ def cpu_baseline(name, nvec, seconds):
     rows = int(max(2000, min(rs.ndets, (seconds - fixed) / per_row)))
     t, rows = rs.step(rows)
     rs.close()
+    threads = rs.threads
     return {"value": rows * nvec / t / 1e9, "unit": "Gdet/s", "cores": threads,
             "kind": "reference",
             "sample": f"reference sigma (diagonal term + compute_cblock_Hfastest), {nvec} "

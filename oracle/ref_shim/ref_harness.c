@@ -319,6 +319,18 @@ double ref_sigma_step_timed(int row0, int nrows, double *diag_s)
 
 void ref_sigma_release(void) { shim_ga_reset(); }
 
+/* OpenMP threads of the reference's parallel regions.  The OMP_NUM_THREADS
+ * variable is read once, when the OpenMP runtime starts, which in a process
+ * that already loaded it (a Python process with torch) is before this
+ * library is loaded; this sets the count directly. */
+#include <omp.h>
+void ref_set_threads(int n)
+{
+        if (n > 0) omp_set_num_threads(n);
+}
+
+int ref_get_threads(void) { return omp_get_max_threads(); }
+
 /* Full reference Davidson solve (pdavidson, pdavidson.c:39) run in
  * directory `workdir` (it writes civec / ci.restart / hvvec there).  On
  * return civec_out holds the nroots result vectors (vector-major) read back
