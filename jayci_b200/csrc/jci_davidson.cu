@@ -16,11 +16,14 @@
 //    processes several vectors and every root converges together.
 // Precision: JCI_FP64, or JCI_MIXED = FP32 sigma (FP32 storage and
 // accumulation) until the residual norms drop below switch_tol, then the
-// basis is collapsed to the krymin lowest Ritz vectors, their sigma vectors
-// are recomputed in FP64 and the iterations continue in FP64 to restol.
-// With block = 0 the mixed schedule takes every root below switch_tol
-// before switching (two root-sequential phases) and rotates sigma vectors
-// with the Ritz coefficients at a collapse instead of recomputing them.
+// basis is collapsed to the krymin lowest Ritz vectors and their sigma
+// vectors are recomputed in FP64.  With block = 0 the mixed schedule takes
+// every root below switch_tol before switching (two root-sequential
+// phases), rotates sigma vectors with the Ritz coefficients at a collapse
+// instead of recomputing them, and refines after the switch with FP32
+// sigma for the new correction vectors and an FP64 sigma of the current
+// root's Ritz vector at every stop (run_sequential); with block = 1 the
+// iterations after the switch run in FP64.
 // Basis vectors, Gram-Schmidt, residuals, the Hdiag preconditioner, the
 // Rayleigh-Ritz eigensolve and the energies are FP64 throughout.
 #include <algorithm>
@@ -1051,6 +1054,48 @@ static jci_status graph_iterations(Ctx &c, const jci_davidson_opts *o, bool fp32
     return JCI_OK;
 }
 
+// Residual norm of root croot in the current subspace, on the host path:
+// r = sum_i y_i (c_i - theta v_i).
+static jci_status residual_norm(Ctx &c, int ckdim, int croot, const std::vector<double> &w,
+                                const std::vector<double> &Y, double *rn) {
+    DavidsonBuffers *b = c.b;
+    std::vector<double> yc(kMaxKry), ycv(kMaxKry);
+    const double th = w[croot - 1];
+    for (int i = 0; i < ckdim; i++) {
+        yc[i] = Y[(croot - 1) * kMaxKry + i];
+        ycv[i] = -th * yc[i];
+    }
+    jci_status r = lincomb(c, b->r, b->C, yc.data(), ckdim, b->V, ycv.data(), ckdim);
+    if (r) return r;
+    double rn2 = 0.0;
+    if ((r = dots(c, b->r, 1, b->r, &rn2))) return r;
+    *rn = sqrt(rn2);
+    return JCI_OK;
+}
+
+// Anchor of the mixed refinement phase: collapse the basis to the kmin
+// lowest Ritz vectors (sigma vectors rotated with them), recompute the
+// sigma of basis vectors [r0, r1) -- the Ritz vectors of the roots being
+// refined -- in FP64, and rebuild the subspace matrix and the Ritz pairs.
+static jci_status anchor(Ctx &c, int &ckdim, int kmin, int r0, int r1, std::vector<double> &G,
+                         std::vector<double> &w, std::vector<double> &Y) {
+    jci_status r;
+    if ((r = collapse(c, ckdim, kmin, Y, true))) return r;
+    ckdim = kmin;
+    if ((r = sigma_block(c, r0, r1 - r0, false))) return r;
+    if ((r = gram_rows(c, 0, ckdim, G))) return r;
+    return rayleigh_ritz(c, ckdim, G, w, Y);
+}
+
+// Residual reduction asked of the FP32-sigma corrections between two
+// anchors of the mixed refinement phase.  A correction's FP32 sigma carries
+// an error of about 1e-6 ||H|| per unit vector, but it enters the current
+// root's residual only through that correction's coefficient in the Ritz
+// vector, which is of the order of the residual at the last anchor divided
+// by the gap to the next root; two decades per anchor stay well above that
+// floor.
+constexpr double kRefineStep = 1e-2;
+
 static jci_status run_sequential(Ctx &c, const jci_davidson_opts *o, bool mixed,
                                  std::vector<double> &w, std::vector<double> &Y, int &ckdim,
                                  int &citer, int &converged, double &rnorm) {
@@ -1062,15 +1107,25 @@ static jci_status run_sequential(Ctx &c, const jci_davidson_opts *o, bool mixed,
     // coefficients instead (the same vectors in exact arithmetic).
     const bool recompute = !mixed;
     // Mixed: phase 1 takes every root, one after the other, below
-    // switch_tol with FP32 sigma; phase 2 collapses to the krymin lowest
-    // Ritz vectors, recomputes their sigma in FP64 and refines every root
-    // from the first to restol.
+    // switch_tol with FP32 sigma.  The switch collapses to the krymin lowest
+    // Ritz vectors and recomputes their sigma in FP64.  Phase 2 refines the
+    // roots from the first to restol: new correction vectors keep FP32
+    // sigma, and every stop of the graph-driven iterations (the current
+    // root's residual below its step target, or a full basis) anchors that
+    // root -- collapse, FP64 sigma of its Ritz vector, new subspace matrix
+    // -- so its residual is measured again with FP64 sigma.  A root counts
+    // as converged only on a residual taken right after its anchor; at the
+    // end every root's Ritz vector gets an FP64 sigma and every residual is
+    // checked again.
     double tol = mixed ? o->switch_tol : o->restol;
+    bool refine = false;
     int croot = 1, cflag = 0;
     bool have_sigma = false;
     ckdim = kmin;
     citer = 1;
     jci_status r;
+    // step target of root k in phase 2 from its residual rn
+    auto target = [&](double rn) { return std::max(o->restol, rn * kRefineStep); };
     while (citer < o->maxiter && croot <= nroots) {
         if (recompute || !have_sigma) {
             if ((r = sigma_block(c, 0, ckdim, fp32))) return r;
@@ -1089,22 +1144,59 @@ static jci_status run_sequential(Ctx &c, const jci_davidson_opts *o, bool mixed,
                 if (r) return r;
             }
             if (event == 0) continue;
+            if (refine) {
+                if ((r = anchor(c, ckdim, kmin, croot - 1, croot, G, w, Y))) return r;
+                double rn = 0.0;
+                if ((r = residual_norm(c, ckdim, croot, w, Y, &rn))) return r;
+                rnorm = rn;
+                if (rn < o->restol) {
+                    if (croot < nroots) {
+                        croot++;
+                        if ((r = residual_norm(c, ckdim, croot, w, Y, &rn))) return r;
+                    } else {
+                        // every root: FP64 sigma of its Ritz vector, residual again
+                        if ((r = anchor(c, ckdim, kmin, 0, nroots, G, w, Y))) return r;
+                        int bad = 0;
+                        for (int k = 1; k <= nroots && !bad; k++) {
+                            if ((r = residual_norm(c, ckdim, k, w, Y, &rn))) return r;
+                            rnorm = std::max(rnorm, rn);
+                            if (rn >= o->restol) bad = k;
+                        }
+                        if (!bad) {
+                            // leave the Ritz vectors of this last eigensolve in
+                            // the basis, as a collapse does
+                            if ((r = collapse(c, ckdim, kmin, Y, true))) return r;
+                            ckdim = kmin;
+                            cflag = 2;
+                            break;
+                        }
+                        croot = bad;
+                    }
+                }
+                tol = target(rn);
+                if (citer >= o->maxiter) break;
+                continue;
+            }
             if (event == 2) {
                 cflag = 0;
                 break;
             }
             cflag = croot < nroots ? 1 : 2;
             if (cflag == 2 && fp32) {
-                fp32 = false;
-                tol = o->restol;
+                refine = true;
                 croot = 1;
                 cflag = 0;
                 if ((r = switch_to_fp64(c, ckdim, kmin, G, w, Y))) return r;
+                double rn = 0.0;
+                if ((r = residual_norm(c, ckdim, croot, w, Y, &rn))) return r;
+                tol = target(rn);
                 continue;
             }
             if (cflag == 1) croot++;
             break;
         }
+        if (cflag == 2 && refine) break;
+        if (refine) break;  // maxiter reached inside the refinement phase
         if ((r = collapse(c, ckdim, kmin, Y, !recompute))) return r;
         ckdim = kmin;
         if (cflag == 2) break;

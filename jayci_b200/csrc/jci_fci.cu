@@ -57,6 +57,7 @@ struct FciTables {
     uint32_t *sortB = nullptr;     // [Ib][f] beta singles sorted by target
     AbTables ab[2];                // fused product's entry lists, 8 / 16 column threads
     GroupTables grp[2];            // same-spin doubles by string groups, per spin
+    int *tc_status = nullptr;      // set by the tcgen05 product if a bounded wait expired
 };
 
 bool fci_supported(const jci_space *s) {
@@ -76,6 +77,7 @@ void fci_free(DeviceState *d) {
         cudaFree(f->sbuf[s]);
     }
     cudaFree(f->sortB);
+    cudaFree(f->tc_status);
     ab_tables_free(&f->ab[0]);
     ab_tables_free(&f->ab[1]);
     group_tables_free(&f->grp[0]);
@@ -885,6 +887,8 @@ jci_status fci_prepare(jci_space *s) {
             JCI_CUDA(cudaMemcpy(f->sortB, so.data(), so.size() * sizeof(uint32_t),
                                 cudaMemcpyHostToDevice));
         }
+        JCI_CUDA(cudaMalloc(&f->tc_status, sizeof(int)));
+        JCI_CUDA(cudaMemset(f->tc_status, 0, sizeof(int)));
     }
     for (int sp = 0; sp < 2; sp++) {
         const SpinTables &t = d->t[sp];
@@ -1075,14 +1079,23 @@ static jci_status launch_mixed2(jci_space *s, const FciArgs<T> &fa, const T *v, 
     return JCI_OK;
 }
 
+// Product engines of the fused plans (4, 5, 7): tx = 8 or 16 column threads
+// of jci_fci_ab.cu, or 32 / 64 = the FP32 tcgen05 engine (jci_fci_tc.cu) with
+// chunks of that many columns.
+static bool is_tc_engine(int tx) { return tx == 32 || tx == 64; }
+// Column threads whose entry lists an engine reads (chunks of 4 tx columns).
+static int ab_table_tx(int tx) { return is_tc_engine(tx) ? tx / 4 : tx; }
+
 static bool ab_plan_possible(const FciTables *f, int tx, size_t w) {
     const AbShape sh{f->nb, f->sa, f->sb, f->nelb, f->npair};
+    if (is_tc_engine(tx)) return w == sizeof(float) && tc_possible(sh, tx, f->smem_max);
     return ab_possible(sh, tx, w, f->smem_max);
 }
 
 // Entry lists of the fused product with tx column threads, built on first use
 // (not while a stream is being captured).
 static jci_status ab_tables(jci_space *s, int tx, cudaStream_t st, AbTables **out) {
+    if (tx != 8 && tx != 16) return JCI_ERR_ARG;
     FciTables *f = s->dev->fci;
     AbTables &t = f->ab[tx == 16 ? 1 : 0];
     if (!t.ent) {
@@ -1101,7 +1114,8 @@ template <typename T>
 static jci_status launch_ab(jci_space *s, const FciArgs<T> &fa, const T *v, T *o,
                             cudaStream_t st, int tx) {
     AbTables *t = nullptr;
-    jci_status r = ab_tables(s, tx, st, &t);
+    const bool tc = is_tc_engine(tx);
+    jci_status r = ab_tables(s, ab_table_tx(tx), st, &t);
     if (r) return r;
     AbArgs<T> m;
     m.na = fa.na; m.nb = fa.nb; m.sa = fa.sa; m.npair = fa.npair; m.mrows = fa.npair + 1;
@@ -1112,6 +1126,12 @@ static jci_status launch_ab(jci_space *s, const FciArgs<T> &fa, const T *v, T *o
     m.fsA = fa.fsA; m.fpA = fa.fpA; m.a1A = fa.a1A; m.m2 = fa.m2;
     m.off = t->off; m.base = t->base; m.ent = t->ent;
     m.skip = fa.skip;
+    if constexpr (sizeof(T) == sizeof(float)) {
+        if (tc) {
+            return tc_launch(m, tx, s->dev->device, v, o, s->dev->fci->tc_status, st);
+        }
+    }
+    if (tc) return JCI_ERR_ARG;
     return ab_launch<T>(m, tx, s->dev->device, v, o, st);
 }
 
@@ -1329,7 +1349,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
             float ms = timeit([&] { return launch_mixed2<T>(s, ar, v, o, st, R); });
             if (ms < bmix2) { bmix2 = ms; Rmix2 = R; }
         }
-    for (int tx : {8, 16}) {
+    for (int tx : {8, 16, 32, 64}) {
         if (!ab_plan_possible(f, tx, w)) continue;
         float ms = timeit([&] { return launch_ab<T>(s, ar, v, o, st, tx); });
         if (ms < bab) { bab = ms; txab = tx; }
@@ -1563,7 +1583,7 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, 
     }
     if (mode == 4 || mode == 5 || mode == 7) {  // tables are built here, outside any capture
         AbTables *t = nullptr;
-        jci_status r = ab_tables(s, R, s->dev->stream, &t);
+        jci_status r = ab_tables(s, ab_table_tx(R), s->dev->stream, &t);
         if (r) return r;
     }
     if (mode == 6 || mode == 7) {

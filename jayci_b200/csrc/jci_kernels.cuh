@@ -51,6 +51,13 @@ void ab_tables_free(AbTables *t);
 template <typename T>
 jci_status ab_launch(const AbArgs<T> &a, int tx, int device, const T *v, T *o,
                      cudaStream_t st);
+// The FP32 fused product on tcgen05 tensor cores (jci_fci_tc.cu), chunk width
+// cw = 32 or 64 (the entry lists of tx = cw / 4).  status (device int,
+// nullable) is set to 1 if a bounded wait of the kernel expired.
+size_t tc_smem(const AbShape &sh, int cw);
+bool tc_possible(const AbShape &sh, int cw, size_t smem_max);
+jci_status tc_launch(const AbArgs<float> &a, int cw, int device, const float *v, float *o,
+                     int *status, cudaStream_t st);
 
 // Same-spin doubles over groups of consecutive strings, jci_fci_group.cu.
 constexpr int kGroupRows = 16;
