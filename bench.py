@@ -270,11 +270,32 @@ class RefSigma:
 
 def calibrate(rs, small, large):
     """The reference's fixed cost per call (buffer setup, whole-vector gets
-    and reductions) and its cost per row, from one block of each size."""
+    and reductions) and its cost per row, from one block of each size after
+    an untimed call of the small one (the first call also pays the page
+    faults of the reference's full-length buffers).  When the two times do
+    not separate (noise larger than the rows' cost), the per-row cost is
+    bounded from above by the large block's time per row and the fixed cost
+    taken as zero, so a sample sized from them never runs long."""
+    rs.step(small)
     t1, r1 = rs.step(small)
     t2, r2 = rs.step(large)
-    per_row = max((t2 - t1) / max(r2 - r1, 1), 1e-12)
+    per_row = (t2 - t1) / max(r2 - r1, 1)
+    if not (t2 > 1.2 * t1 and per_row > 0):
+        return 0.0, t2 / r2
     return max(t1 - per_row * r1, 0.0), per_row
+
+
+def sample_rows(fixed, per_row, seconds, large, ndets):
+    """Rows of a sample of about `seconds` of reference work: at least 2000,
+    at most 64 times the largest calibrated block, at most every row."""
+    rows = (seconds - fixed) / per_row if seconds > fixed else 2000
+    return int(max(2000, min(ndets, 64 * large, rows)))
+
+
+def calib_sizes(ndets):
+    """Calibration blocks: 2000 rows and about 0.1% of the rows (at least
+    20000), so the large one is well above the fixed cost at every size."""
+    return 2000, max(20000, ndets // 1000)
 
 
 def run_reference(a):
@@ -295,13 +316,14 @@ def run_reference(a):
     os.environ["OMP_NUM_THREADS"] = str(threads)
     os.environ.setdefault("OMP_SCHEDULE", "dynamic,64")
     rs = RefSigma(a.workload, nroots)
-    # warm-up steps: the first two calibrate the fixed cost and the per-row
-    # cost; every timed step then runs the block that fits its time share
-    fixed, per_row = calibrate(rs, 2000, 20000)
-    for _ in range(max(0, a.warmup - 2)):
-        rs.step(2000)
+    # warm-up steps: the first three calibrate the fixed cost and the
+    # per-row cost; every timed step then runs the block that fits its share
+    small, large = calib_sizes(rs.ndets)
+    fixed, per_row = calibrate(rs, small, large)
+    for _ in range(max(0, a.warmup - 3)):
+        rs.step(small)
     budget = a.ref_seconds / max(a.steps, 1)
-    rows = int(max(2000, min(rs.ndets, (budget - fixed) / per_row)))
+    rows = sample_rows(fixed, per_row, budget, large, rs.ndets)
     times, done = [], 0
     for _ in range(a.steps):
         t, r = rs.step(rows)
@@ -323,8 +345,9 @@ def run_reference(a):
            "reference_cost_model": {
                "fixed_s_per_call": fixed, "s_per_row": per_row,
                "extrapolated_full_sigma_s": fixed + per_row * ndets,
-               "note": "fixed cost and per-row cost from two calibration blocks "
-                       "(2000 and 20000 rows); the full-sigma time is an extrapolation"},
+               "note": f"fixed cost and per-row cost from two calibration blocks "
+                       f"({small} and {large} rows, after an untimed call); the "
+                       f"full-sigma time is an extrapolation"},
            "cpu_baseline": {"value": value, "unit": "Gdet/s", "cores": threads,
                             "kind": "reference", "sample": sample},
            "e2e": {"value": value, "unit": "Gdet/s", "h2d_bytes_per_step": 0,
@@ -347,8 +370,9 @@ def cpu_baseline(name, nvec, seconds):
     threads = host_threads(ndets, nvec)
     os.environ["OMP_NUM_THREADS"] = str(threads)
     rs = RefSigma(name, nvec)
-    fixed, per_row = calibrate(rs, 2000, 20000)
-    rows = int(max(2000, min(rs.ndets, (seconds - fixed) / per_row)))
+    small, large = calib_sizes(rs.ndets)
+    fixed, per_row = calibrate(rs, small, large)
+    rows = sample_rows(fixed, per_row, seconds, large, rs.ndets)
     t, rows = rs.step(rows)
     rs.close()
     threads = rs.threads

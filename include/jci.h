@@ -159,7 +159,8 @@ jci_status jci_sigma(jci_space *s, int nvec, const double *v, double *sigma,
 
 /* Same on device memory: nvec vectors with leading dimension ld (>= ndets,
  * elements); element type double for JCI_FP64, float for JCI_FP32.  The
- * work is queued on `stream` (a cudaStream_t, NULL = default stream). */
+ * work is queued on `stream` (a cudaStream_t; NULL = the handle's own
+ * stream, not the legacy default stream). */
 jci_status jci_sigma_device(jci_space *s, int nvec, const void *v,
                             void *sigma, long long ld, int precision,
                             void *stream);

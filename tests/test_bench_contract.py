@@ -97,6 +97,22 @@ def test_reference_calibration_separates_fixed_and_row_costs():
             return 4.0 + 1e-3 * rows, rows
     fixed, per_row = bench.calibrate(Fake(), 2000, 20000)
     assert abs(fixed - 4.0) < 1e-9 and abs(per_row - 1e-3) < 1e-12
+    assert bench.sample_rows(fixed, per_row, 15.0, 20000, 10 ** 9) == 11000
+
+
+def test_reference_calibration_is_bounded_when_noise_hides_the_rows():
+    class Noisy:
+        """Fixed cost 3 s with noise larger than the rows' cost: the second
+        call, with ten times the rows, comes out faster."""
+        def __init__(self):
+            self.t = iter([5.0, 3.2, 3.1])
+        def step(self, rows):
+            return next(self.t), rows
+    fixed, per_row = bench.calibrate(Noisy(), 2000, 165636)
+    assert fixed == 0.0 and per_row == 3.1 / 165636
+    rows = bench.sample_rows(fixed, per_row, 15.0, 165636, 165636900)
+    assert rows <= 64 * 165636 and rows * per_row <= 15.0 + 1e-9
+    assert bench.calib_sizes(165636900) == (2000, 165636)
 
 
 def test_reference_threads_are_bounded_by_memory():
