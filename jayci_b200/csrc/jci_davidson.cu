@@ -278,8 +278,30 @@ __global__ void k_lincomb(double *__restrict__ out, long long n, long long ld,
     for (int i = threadIdx.x; i < mx; i += blockDim.x) ca[i] = a[i];
     for (int i = threadIdx.x; i < my; i += blockDim.x) cb[i] = b[i];
     __syncthreads();
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-         k += (long long)gridDim.x * blockDim.x) {
+    // element pairs with 16-byte loads (ld is a multiple of 32 and the panels
+    // 256-byte aligned, so every pair is aligned); the same sums, in the same
+    // order, as one element at a time
+    const long long n2 = n / 2;
+    for (long long k2 = (long long)blockIdx.x * blockDim.x + threadIdx.x; k2 < n2;
+         k2 += (long long)gridDim.x * blockDim.x) {
+        const long long k = 2 * k2;
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll 4
+        for (int i = 0; i < mx; i++) {
+            const double2 x = *reinterpret_cast<const double2 *>(X + i * ld + k);
+            s0 += ca[i] * x.x;
+            s1 += ca[i] * x.y;
+        }
+#pragma unroll 4
+        for (int i = 0; i < my; i++) {
+            const double2 y = *reinterpret_cast<const double2 *>(Y + i * ld + k);
+            s0 += cb[i] * y.x;
+            s1 += cb[i] * y.y;
+        }
+        *reinterpret_cast<double2 *>(out + k) = make_double2(s0, s1);
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const long long k = n - 1;
         double s = 0.0;
         for (int i = 0; i < mx; i++) s += ca[i] * X[i * ld + k];
         for (int i = 0; i < my; i++) s += cb[i] * Y[i * ld + k];
@@ -298,8 +320,21 @@ __global__ void k_orth_update(double *__restrict__ t, long long n, long long ld,
     __shared__ double c[kMaxKry];
     for (int i = threadIdx.x; i < m; i += blockDim.x) c[i] = ov[i];
     __syncthreads();
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-         k += (long long)gridDim.x * blockDim.x) {
+    const long long n2 = n / 2;  // element pairs, 16-byte loads (as k_lincomb)
+    for (long long k2 = (long long)blockIdx.x * blockDim.x + threadIdx.x; k2 < n2;
+         k2 += (long long)gridDim.x * blockDim.x) {
+        const long long k = 2 * k2;
+        double2 s = *reinterpret_cast<const double2 *>(t + k);
+#pragma unroll 4
+        for (int i = 0; i < m; i++) {
+            const double2 x = *reinterpret_cast<const double2 *>(X + i * ld + k);
+            s.x -= c[i] * x.x;
+            s.y -= c[i] * x.y;
+        }
+        *reinterpret_cast<double2 *>(t + k) = s;
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const long long k = n - 1;
         double s = t[k];
         for (int i = 0; i < m; i++) s -= c[i] * X[i * ld + k];
         t[k] = s;

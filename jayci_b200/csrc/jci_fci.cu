@@ -1304,16 +1304,25 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     JCI_CUDA(cudaEventCreate(&e0));
     JCI_CUDA(cudaEventCreate(&e1));
     jci_status err = JCI_OK;
-    // ms per call of fn (one untimed call, then two timed)
+    // ms per call of fn: one untimed call, then two timed -- or one, when a
+    // call takes more than 50 ms (large spaces: launch noise is then far
+    // below the differences between candidates, and tuning time matters)
     auto timeit = [&](auto fn) -> float {
         if (err || (err = fn())) return 1e30f;
-        cudaEventRecord(e0, st);
-        for (int k = 0; k < 2 && !err; k++) err = fn();
-        cudaEventRecord(e1, st);
-        cudaEventSynchronize(e1);
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        return err ? 1e30f : ms / 2;
+        int reps = 0;
+        for (int k = 0; k < 2 && !err; k++) {
+            cudaEventRecord(e0, st);
+            err = fn();
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            ms += t;
+            reps++;
+            if (t > 50.f) break;
+        }
+        return err ? 1e30f : ms / reps;
     };
     auto useful = [&](int nt) {
         int items = (f->nb + nt - 1) / nt;
@@ -1439,7 +1448,10 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     // configuration end to end before choosing
     auto best_of = [&](auto fn) {
         float m = 1e30f;
-        for (int k = 0; k < 3; k++) m = std::min(m, timeit(fn));
+        for (int k = 0; k < 3; k++) {
+            m = std::min(m, timeit(fn));
+            if (m > 50.f && m < 1e29f) break;  // as in timeit
+        }
         return m;
     };
     if (b0nt) best0 = best_of([&] { return run_plan<T>(s, a, 0, b0nt, b0R, 1, v, o, st); });

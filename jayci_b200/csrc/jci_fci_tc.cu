@@ -15,24 +15,29 @@
 // x_h = tf32(x), x_l = tf32(x - x_h), and each tile takes
 // A_l B_h + A_h B_l + A_h B_h with FP32 accumulation in tensor memory.
 //
-// Per chunk the CTA (256 or 512 threads) works as a pipeline over two B buffers and
-// two tensor-memory accumulators:
-//   1. all threads stage B(c+1) = rows Ja_j of C, columns of chunk c+1, split
-//      into TF32 high and low parts, in the K-major core-matrix layout the
-//      MMA reads (8 rows x 16 bytes per core matrix, no swizzle);
+// Per chunk the CTA (512 threads) works as a pipeline over two B buffers and
+// two tensor-memory accumulators; in step c:
+//   1. all threads split B(c+1) -- rows Ja_j of C, columns of chunk c+1,
+//      copied raw one step earlier -- in place into TF32 high and low parts,
+//      in the K-major core-matrix layout the MMA reads (8 rows x 16 bytes
+//      per core matrix, no swizzle);
 //   2. one thread issues the MMAs of chunk c+1 (3 x K8/8 tcgen05.mma of
-//      128 x CW x 8 per 128-row tile) and commits them to an mbarrier;
-//   3. the chunk's entry lists arrive by cp.async.bulk on another mbarrier;
-//   4. all threads wait for chunk c's MMAs, move the accumulator tensor
-//      memory -> registers -> shared memory (tcgen05.ld), and gather.
-// The MMAs of chunk c+1 therefore run under the B staging and the gather of
-// chunk c.  Every wait is bounded (about one second of global time); on
+//      128 x CW x 8 per 128-row tile), committed to an mbarrier, and the
+//      bulk copy (cp.async.bulk) of chunk c's entry lists;
+//   3. all threads wait for chunk c's MMAs; its B buffer takes the raw copy
+//      (cp.async) of B(c+2) at once, and its accumulator moves tensor
+//      memory -> registers -> shared memory (tcgen05.ld);
+//   4. all threads gather chunk c.
+// Chunk c+1's MMAs run under chunk c's extraction and gather, and B(c+2)'s
+// copies land under them too.  Every wait is bounded (about one second of global time); on
 // expiry the kernel records an error, leaves the remaining work, waits (also
 // bounded) for its committed MMAs and releases its tensor memory.
 //
 // Shared memory (bytes, K8 = alpha singles rounded up to 8, MT 128-row tiles):
 //   A_h, A_l  2 x MT x 128 x K8 x 4     B_h, B_l  2 buffers x 2 x CW x K8 x 4
 //   T         mrows x (CW + 4) x 4      lists     maxent x 4 + offs x 2
+#include <cuda_pipeline.h>
+
 #include <algorithm>
 #include <cstdint>
 
@@ -244,26 +249,39 @@ __global__ void __launch_bounds__(NT, 1)
     int issued[2] = {0, 0}, lists = 0;
     bool failed = false;
 
-    // B chunk c into buffer b: rows Ja_j of C, TF32 high and low parts.
-    auto stage_b = [&](int c, int b) {
+    // Raw B chunk c into buffer b: rows Ja_j of C, the chunk's columns, as
+    // plain FP32 values at their places in the high-part tile (one 4-byte
+    // cp.async each: a core-matrix row holds 4 consecutive k of one column).
+    // Rows k >= K and columns past nb are zeros written directly.
+    auto fetch_b = [&](int c, int b) {
         const int c0 = c * CW;
+        const uint32_t bh = L.bh + (uint32_t)b * L.bstride;
+        for (int idx = tid; idx < CW * K8; idx += NT) {
+            const int n = idx % CW, k = idx / CW, col = c0 + n;
+            float *dst = reinterpret_cast<float *>(smem + bh + tc_off(n, k, K8));
+            if (k < K && col < nb)
+                __pipeline_memcpy_async(dst, V + (long long)jl[k] * nb + col, 4);
+            else
+                *dst = 0.f;
+        }
+        __pipeline_commit();
+    };
+    // Split the landed raw chunk in buffer b in place: high part stays,
+    // remainder to the low-part tile.
+    auto split_b = [&](int b) {
         const uint32_t bh = L.bh + (uint32_t)b * L.bstride, bl = L.bl + (uint32_t)b * L.bstride;
         for (int idx = tid; idx < CW * (K8 / 4); idx += NT) {
-            const int n = idx % CW, kq = idx / CW, col = c0 + n;
-            float x[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const int k = 4 * kq + u;
-                x[u] = (k < K && col < nb) ? V[(long long)jl[k] * nb + col] : 0.f;
-            }
+            const uint32_t o = 16u * (uint32_t)idx;  // the tile is CW * K8 / 4 pieces of 16 bytes
+            uint4 x = *reinterpret_cast<const uint4 *>(smem + bh + o);
             uint4 hi, lo;
+            const uint32_t *xv = &x.x;
             uint32_t *h = &hi.x, *l = &lo.x;
 #pragma unroll
             for (int u = 0; u < 4; u++) {
-                h[u] = tc_tf32(x[u]);
-                l[u] = tc_tf32(x[u] - __uint_as_float(h[u]));
+                const float f = __uint_as_float(xv[u]);
+                h[u] = tc_tf32(f);
+                l[u] = tc_tf32(f - __uint_as_float(h[u]));
             }
-            const uint32_t o = tc_off(n, 4 * kq, K8);
             *reinterpret_cast<uint4 *>(smem + bh + o) = hi;
             *reinterpret_cast<uint4 *>(smem + bl + o) = lo;
         }
@@ -295,19 +313,23 @@ __global__ void __launch_bounds__(NT, 1)
         // A panel of this alpha string (split) and its single targets
         for (int idx = tid; idx < MT * 128 * (K8 / 4); idx += NT) {
             const int m = idx % (MT * 128), kq = idx / (MT * 128);
+            float v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int j = 4 * kq + u;
+                v[u] = 0.f;
+                if (j < K && m <= a.npair) {
+                    const long long o = (long long)j * a.na + Ia;
+                    v[u] = m < a.npair ? a.m2[eri_index(a.fpA[o], m)] : a.a1A[o];
+                    if (a.fsA[o] >> 31) v[u] = -v[u];
+                }
+            }
             uint4 hi, lo;
             uint32_t *h = &hi.x, *l = &lo.x;
 #pragma unroll
             for (int u = 0; u < 4; u++) {
-                const int j = 4 * kq + u;
-                float v = 0.f;
-                if (j < K && m <= a.npair) {
-                    const long long o = (long long)j * a.na + Ia;
-                    v = m < a.npair ? a.m2[eri_index(a.fpA[o], m)] : a.a1A[o];
-                    if (a.fsA[o] >> 31) v = -v;
-                }
-                h[u] = tc_tf32(v);
-                l[u] = tc_tf32(v - __uint_as_float(h[u]));
+                h[u] = tc_tf32(v[u]);
+                l[u] = tc_tf32(v[u] - __uint_as_float(h[u]));
             }
             const int t = m / 128, r = m % 128;
             const uint32_t o = (uint32_t)(t * 128 * K8 * 4) + tc_off(r, 4 * kq, K8);
@@ -316,8 +338,12 @@ __global__ void __launch_bounds__(NT, 1)
         }
         for (int j = tid; j < K; j += NT)
             jl[j] = (int)(a.fsA[(long long)j * a.na + Ia] & 0x3fffffffu);
-        __syncthreads();  // jl before the B staging reads it
-        stage_b(0, 0);
+        __syncthreads();  // jl before the B copies read it
+        fetch_b(0, 0);
+        if (a.nchunk > 1) fetch_b(1, 1);  // the previous string's MMAs are all done
+        __pipeline_wait_prior(a.nchunk > 1 ? 1 : 0);
+        __syncthreads();  // raw B(0) landed (every thread's copies)
+        split_b(0);
         fence_proxy_async();
         tc_fence_before();
         __syncthreads();
@@ -331,10 +357,13 @@ __global__ void __launch_bounds__(NT, 1)
         for (int ci = 0; ci < a.nchunk; ci++) {
             const int b = ci & 1;
             const bool more = ci + 1 < a.nchunk;
-            if (more) stage_b(ci + 1, b ^ 1);
+            __pipeline_wait_prior(0);  // this thread's raw B(ci+1) copies
+            tc_fence_before();
+            __syncthreads();  // raw B(ci+1) landed; gather(ci-1) and its T reads done
+            if (more) split_b(b ^ 1);
             fence_proxy_async();
             tc_fence_before();
-            __syncthreads();  // B(ci+1) staged; gather(ci-1) and T reads of ci-1 done
+            __syncthreads();  // B(ci+1) split
             if (tid == 0) {
                 // the chunk's entry lists, by bulk copy
                 const uint32_t e0 = a.base[ci], ne = a.base[ci + 1] - e0;
@@ -348,13 +377,15 @@ __global__ void __launch_bounds__(NT, 1)
                     issued[b ^ 1]++;
                 }
             }
-            // chunk ci's accumulator -> T in shared memory
+            // chunk ci's MMAs done: its B buffer takes raw B(ci+2) now, and its
+            // accumulator goes to T in shared memory
             bool ok = mbar_wait(bar_mma0 + 8 * b, ph_mma[b]);
             if (ok) {
                 ph_mma[b] ^= 1u;
                 if (tid == 0) issued[b]--;
             }
             tc_fence_after();
+            if (ok && ci + 2 < a.nchunk) fetch_b(ci + 2, b);
             const int wg = warp >> 2, row = 32 * (warp & 3) + lane;
             if (ok && wg < MT) {
                 const int m = 128 * wg + row;
@@ -401,6 +432,7 @@ __global__ void __launch_bounds__(NT, 1)
                 }
             }
         }
+        __pipeline_wait_prior(0);
         if (failed) break;
         float *srow = S + (long long)Ia * nb;
 #pragma unroll
@@ -432,23 +464,24 @@ __global__ void __launch_bounds__(NT, 1)
 
 using TcKernel = void (*)(AbArgs<float>, const float *, float *, int *);
 
-// Threads per CTA and beta strings per thread: 256 threads for up to 4096
-// beta strings (4 or 16 each), 512 threads with 32 each up to 16384 (with
-// 32-column chunks only: the 64-column form would exceed the 128 registers
-// a thread of a 512-thread CTA may hold).
-int tc_threads(int nb) { return nb <= 4096 ? 256 : 512; }
+// 512 threads per CTA (16 warps hide the copy and gather latency of the one
+// CTA an SM holds) and 4, 8, 16 or 32 beta strings per thread, up to 16384
+// beta strings -- 32 per thread with 32-column chunks only: the 64-column
+// form would exceed the 128 registers a thread of a 512-thread CTA may hold.
+constexpr int kTcThreads = 512;
 
 int tc_items(int nb) {
-    const int nt = tc_threads(nb), it = (nb + nt - 1) / nt;
-    return nt == 256 ? (it <= 4 ? 4 : 16) : (it <= 32 ? 32 : 0);
+    const int it = (nb + kTcThreads - 1) / kTcThreads;
+    return it <= 4 ? 4 : it <= 8 ? 8 : it <= 16 ? 16 : it <= 32 ? 32 : 0;
 }
 
 template <int CW, int MT>
 TcKernel tc_kernel_items(int items) {
-    if (items == 4) return k_sigma_ab_tc<256, CW, MT, 4>;
-    if (items == 16) return k_sigma_ab_tc<256, CW, MT, 16>;
+    if (items == 4) return k_sigma_ab_tc<kTcThreads, CW, MT, 4>;
+    if (items == 8) return k_sigma_ab_tc<kTcThreads, CW, MT, 8>;
+    if (items == 16) return k_sigma_ab_tc<kTcThreads, CW, MT, 16>;
     if constexpr (CW == 32) {
-        if (items == 32) return k_sigma_ab_tc<512, CW, MT, 32>;
+        if (items == 32) return k_sigma_ab_tc<kTcThreads, CW, MT, 32>;
     }
     return nullptr;
 }
@@ -487,7 +520,7 @@ jci_status tc_launch(const AbArgs<float> &a, int cw, int device, const float *v,
     TcKernel kern = tc_kernel(cw, mt, items);
     if (!kern || a.nchunk != (a.nb + cw - 1) / cw || a.sa > 64) return JCI_ERR_SPACE;
     const size_t smem = tc_layout(a.sa, mt, cw, a.mrows, a.maxent, a.offs).total;
-    const int nt = tc_threads(a.nb);
+    const int nt = kTcThreads;
     JCI_CUDA(smem_optin(kern));
     int occ = 0, nsm = 0;
     JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nt, smem));
