@@ -78,9 +78,15 @@ def sigma_plan_desc(mode, nt, R, B, ms=None):
     streams, groups = mode in (3, 4), mode in (6, 7)
     d = {"mode": mode, "name": PLAN_NAMES[mode],
          ("alpha_pass_threads" if streams else "beta_singles_threads" if groups
-          else "row_kernel_threads"): nt,
-         ("staged_rows" if mode == 0 else
-          "product_column_threads" if mode in (4, 5, 7) else "product_ctas_per_sm"): R}
+          else "row_kernel_threads"): nt}
+    if mode == 0:
+        d["staged_rows"] = R
+    elif mode in (4, 5, 7):
+        d["product_engine"] = (f"tcgen05 3xTF32, {R}-column chunks" if R in (32, 64) else
+                               f"{R} column threads")
+    else:
+        d["product_ctas_per_sm"] = R % 16
+        d["product_panel"] = "256-column blocks" if R >= 16 else "whole alpha row"
     if groups:
         d["group_kernel"] = (f"{B} column(s) per thread" if B <= 2 else
                              f"targets split over 4 warps, {5 - B} column(s) per lane")
@@ -116,12 +122,22 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def committed_profile(workload, mode, B):
-    """Per-launch figures of sigma plan `mode` on `workload` from the
-    committed ncu summary (profiles/sigma_<workload>_traffic.json), or None
-    when that plan was not captured.  Entries are keyed by mode, and for
-    the string-group plans (6, 7) by mode and group kernel variant ("7:3")."""
+def profile_key(mode, R, B):
+    """Key of a sigma plan in the committed traffic summaries: the mode; for
+    the string-group plans (6, 7) also the group kernel variant ("7:3"); for
+    the panel products (1, 3, 6) a ":blk" suffix when the panel is cut into
+    column blocks (R >= 16)."""
     key = f"{mode}:{B}" if mode in (6, 7) else str(mode)
+    if mode in (1, 3, 6) and R >= 16:
+        key += ":blk"
+    return key
+
+
+def committed_profile(workload, mode, B, R=0):
+    """Per-launch figures of sigma plan (mode, R, B) on `workload` from the
+    committed ncu summary (profiles/sigma_<workload>_traffic.json), or None
+    when that plan was not captured (keys: profile_key)."""
+    key = profile_key(mode, R, B)
     p = os.path.join(ROOT, "profiles", f"sigma_{workload}_traffic.json")
     if os.path.exists(p):
         try:
@@ -550,7 +566,7 @@ def run_gpu(a):
     achieved = bytes_per_launch / avg_launch_s / 1e9
     mode, nt, R, B, tms = sp.sigma_tuning(jb.FP64)
     tune32 = sp.sigma_tuning(jb.FP32)
-    prof = committed_profile(a.workload, mode, B) or {}
+    prof = committed_profile(a.workload, mode, B, R) or {}
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": prof.get("dram_bytes_per_launch"),
             "algorithmic_bytes_per_launch": bytes_per_launch, "peak_source": peak_kind,
@@ -659,14 +675,20 @@ def run_serve(a):
                           0.0, nroots=r["nroots"], warm_from=warm, krymin=kmin, krymax=kmax,
                           **kw)
 
-    def by_size(rows):
+    def by_size(rows, lat=None):
+        """Per size class: solve time, iterations, sigma time (means) and,
+        with lat (queue + solve seconds per row), latency p50 / p99."""
         out = {}
         for m in sorted(set(x[0] for x in rows)):
-            sel = [x for x in rows if x[0] == m]
-            out[f"cas{m}"] = dict(n=len(sel),
-                                  solve_ms=float(np.mean([x[1] for x in sel]) * 1e3),
-                                  iterations=float(np.mean([x[2] for x in sel])),
-                                  sigma_ms=float(np.mean([x[3] for x in sel]) * 1e3))
+            idx = [i for i, x in enumerate(rows) if x[0] == m]
+            sel = [rows[i] for i in idx]
+            d = dict(n=len(sel), solve_ms=float(np.mean([x[1] for x in sel]) * 1e3),
+                     iterations=float(np.mean([x[2] for x in sel])),
+                     sigma_ms=float(np.mean([x[3] for x in sel]) * 1e3))
+            lt = [lat[i] for i in idx] if lat is not None else [x[1] for x in sel]
+            d["p50_ms"] = float(np.percentile(lt, 50) * 1e3)
+            d["p99_ms"] = float(np.percentile(lt, 99) * 1e3)
+            out[f"cas{m}"] = d
         return out
 
     # warm-up: one solve per size class (autotuning, table build)
@@ -734,7 +756,7 @@ def run_serve(a):
                     p50_ms=float(np.percentile(lat, 50) * 1e3),
                     p99_ms=float(np.percentile(lat, 99) * 1e3),
                     warm_started=int(sum(x.warm_started for x in res)), all_converged=ok,
-                    not_converged=failed[:8], by_size=by_size(rows))
+                    not_converged=failed[:8], by_size=by_size(rows, list(lat)))
 
     one = play(1, 0.0)
     rate = 1.5 * one["solves_per_s"]

@@ -58,6 +58,9 @@ struct FciTables {
     AbTables ab[2];                // fused product's entry lists, 8 / 16 column threads
     GroupTables grp[2];            // same-spin doubles by string groups, per spin
     int *tc_status = nullptr;      // set by the tcgen05 product if a bounded wait expired
+    AbTables abk;                  // per-block lists of the column-blocked panel product
+    void *tbufk[2] = {nullptr, nullptr};  // its per-CTA scratch blocks
+    int mixk_grid[2] = {0, 0};
 };
 
 bool fci_supported(const jci_space *s) {
@@ -78,6 +81,9 @@ void fci_free(DeviceState *d) {
     }
     cudaFree(f->sortB);
     cudaFree(f->tc_status);
+    cudaFree(f->tbufk[0]);
+    cudaFree(f->tbufk[1]);
+    ab_tables_free(&f->abk);
     ab_tables_free(&f->ab[0]);
     ab_tables_free(&f->ab[1]);
     group_tables_free(&f->grp[0]);
@@ -393,6 +399,132 @@ __global__ void __launch_bounds__(kMixThreads)
                 x += flip(Tb[(size_t)a.fpB[o] * a.nbp + (e & 0x3fffffffu)], e >> 31);
             }
             srow[Ib] += x;
+        }
+    }
+}
+
+// ---- dense product through a column-blocked panel --------------------------
+//
+// The product of k_sigma_mixed with its panel cut into blocks of kMixBlock
+// columns: the CTA forms T[:, block] (kMixBlock / 64 chunks, as above) in a
+// scratch block of mrows x kMixBlock, then gathers the block's share of every
+// beta string's terms -- the entries of the per-block lists (ab_tables_build
+// with 4 tx = kMixBlock: the one-body row, the Coulomb rows and the singles
+// whose target column lies in the block, in list order) -- and adds it to
+// sigma(Ia, Ib) in place.  The scratch block (FCI(16,16): 137 x 256 x 8 B =
+// 280 KB) and the sigma row stay in L2, where the whole-row panel (14 MB)
+// spilled to DRAM and its gather read it at random.  Sums run block by
+// block, then in list order: bitwise reproducible.
+constexpr int kMixBlock = 256;
+
+template <typename T>
+struct MixBArgs {
+    MixArgs<T> m;
+    int offs;                 // offset row stride of the block lists
+    const uint16_t *off;      // [block][offs]
+    const uint32_t *base;     // [block + 1]
+    const uint32_t *ent;      // col | row << 8 | phase << 31
+};
+
+template <typename T, int TM>
+__global__ void __launch_bounds__(kMixThreads)
+    k_sigma_mixed_blk(MixBArgs<T> ab, const T *__restrict__ V, T *__restrict__ S,
+                      T *__restrict__ Tbuf) {
+    const MixArgs<T> &a = ab.m;
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int MP = 16 * TM;
+    constexpr int CPB = kMixBlock / kMixCols;  // chunks per block
+    const int K = a.sa;
+    T *As = reinterpret_cast<T *>(smem_raw);          // [K][MP]
+    T *Bs = As + (size_t)K * MP;                      // [2][K][64]
+    int *jl = reinterpret_cast<int *>(Bs + 2 * (size_t)K * kMixCols);  // [K]
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    T *Tb = Tbuf + (size_t)blockIdx.x * a.mrows * kMixBlock;
+    const int nchunk = a.nbp / kMixCols;
+    auto stage = [&](int c, T *buf) {
+        const int c0 = c * kMixCols;
+        for (int idx = tid; idx < K * kMixCols; idx += kMixThreads) {
+            int j = idx >> 6, col = c0 + (idx & 63);
+            if (col < a.nb)
+                __pipeline_memcpy_async(buf + idx, V + (long long)jl[j] * a.nb + col, sizeof(T));
+            else
+                buf[idx] = T(0);
+        }
+        __pipeline_commit();
+    };
+    for (int Ia = blockIdx.x; Ia < a.na; Ia += gridDim.x) {
+        __syncthreads();
+        for (int idx = tid; idx < K * MP; idx += kMixThreads) {
+            int j = idx / MP, m = idx - j * MP;
+            long long o = (long long)j * a.na + Ia;
+            uint32_t e = a.fsA[o];
+            T v = T(0);
+            if (m < a.npair) v = a.m2[eri_index(a.fpA[o], m)];
+            else if (m == a.npair) v = a.a1A[o];
+            As[idx] = flip(v, e >> 31);
+            if (m == 0) jl[j] = (int)(e & 0x3fffffffu);
+        }
+        __syncthreads();
+        T *srow = S + (long long)Ia * a.nb;
+        stage(0, Bs);
+        for (int ci = 0; ci < nchunk; ci++) {
+            const int cb = ci % CPB;
+            T *Bc = Bs + (size_t)(ci & 1) * K * kMixCols;
+            if (ci + 1 < nchunk) {
+                stage(ci + 1, Bs + (size_t)((ci + 1) & 1) * K * kMixCols);
+                __pipeline_wait_prior(1);
+            } else {
+                __pipeline_wait_prior(0);
+            }
+            __syncthreads();
+            T acc[TM][4];
+#pragma unroll
+            for (int i = 0; i < TM; i++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) acc[i][q] = T(0);
+#pragma unroll 4
+            for (int k = 0; k < K; k++) {
+                const T *br = Bc + k * kMixCols + tx;
+                T b0 = br[0], b1 = br[16], b2 = br[32], b3 = br[48];
+                const T *ar = As + k * MP + ty * TM;
+#pragma unroll
+                for (int i = 0; i < TM; i++) {
+                    T av = ar[i];
+                    acc[i][0] = fma(av, b0, acc[i][0]);
+                    acc[i][1] = fma(av, b1, acc[i][1]);
+                    acc[i][2] = fma(av, b2, acc[i][2]);
+                    acc[i][3] = fma(av, b3, acc[i][3]);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < TM; i++) {
+                int m = ty * TM + i;
+                if (m < a.mrows) {
+                    T *dst = Tb + (size_t)m * kMixBlock + cb * kMixCols + tx;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) dst[16 * q] = acc[i][q];
+                }
+            }
+            if (cb == CPB - 1 || ci + 1 == nchunk) {
+                // the block is complete: gather its terms into sigma(Ia, :)
+                __syncthreads();
+                const int blk = ci / CPB;
+                const uint16_t *off = ab.off + (size_t)blk * ab.offs;
+                const uint32_t *ent = ab.ent + ab.base[blk];
+                for (int Ib = tid; Ib < a.nb; Ib += kMixThreads) {
+                    const int k0 = off[Ib], k1 = off[Ib + 1];
+                    if (k0 == k1) continue;
+                    T x = T(0);
+                    for (int k = k0; k < k1; k++) {
+                        const uint32_t e = ent[k];
+                        x += flip(Tb[(size_t)((e >> 8) & 0xffffu) * kMixBlock + (e & 0xffu)],
+                                  e >> 31);
+                    }
+                    srow[Ib] += x;
+                }
+            }
+            __syncthreads();
         }
     }
 }
@@ -988,10 +1120,68 @@ static bool mixed_possible(const FciTables *f, size_t w) {
     return TM <= 9 && f->sa >= 1 && mix_smem(f->sa, TM, w) <= f->smem_max;
 }
 
+static jci_status ab_tables(jci_space *s, int tx, cudaStream_t st, AbTables **out);
+
+template <typename T, int TM>
+static jci_status launch_mixed_blk_t(jci_space *s, const MixBArgs<T> &ab, const T *v, T *o,
+                                     cudaStream_t st, int per_sm) {
+    DeviceState *d = s->dev;
+    FciTables *f = d->fci;
+    const int prec = sizeof(T) == 8 ? 0 : 1;
+    auto kern = k_sigma_mixed_blk<T, TM>;
+    size_t smem = mix_smem(ab.m.sa, TM, sizeof(T));
+    JCI_CUDA(smem_optin(kern));
+    int occ = 0, nsm = 0;
+    JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kMixThreads, smem));
+    JCI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d->device));
+    occ = std::max(occ, 1);
+    if (!f->mixk_grid[prec]) {  // scratch blocks for the largest resident grid, once
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        JCI_CUDA(cudaStreamIsCapturing(st, &cs));
+        if (cs != cudaStreamCaptureStatusNone) return JCI_ERR_STATE;
+        const int g = std::max(1, std::min(ab.m.na, nsm * occ));
+        JCI_CUDA(cudaMalloc(&f->tbufk[prec], (size_t)g * ab.m.mrows * kMixBlock * sizeof(T)));
+        f->mixk_grid[prec] = g;
+    }
+    int grid = f->mixk_grid[prec];
+    if (per_sm > 0 && per_sm < occ) grid = std::max(1, std::min(grid, nsm * per_sm));
+    kern<<<grid, kMixThreads, smem, st>>>(ab, v, o, (T *)f->tbufk[prec]);
+    return JCI_OK;
+}
+
+// The product through the column-blocked panel (k_sigma_mixed_blk) with
+// per_sm CTAs per SM (0 = as many as fit).
+template <typename T>
+static jci_status launch_mixed_blk(jci_space *s, const MixArgs<T> &m, const T *v, T *o,
+                                   cudaStream_t st, int per_sm) {
+    AbTables *t = nullptr;
+    jci_status r = ab_tables(s, kMixBlock / 4, st, &t);
+    if (r) return r;
+    MixBArgs<T> ab;
+    ab.m = m;
+    ab.offs = t->offs;
+    ab.off = t->off;
+    ab.base = t->base;
+    ab.ent = t->ent;
+    switch ((m.mrows + 15) / 16) {
+        case 1: return launch_mixed_blk_t<T, 1>(s, ab, v, o, st, per_sm);
+        case 2: return launch_mixed_blk_t<T, 2>(s, ab, v, o, st, per_sm);
+        case 3: return launch_mixed_blk_t<T, 3>(s, ab, v, o, st, per_sm);
+        case 4: return launch_mixed_blk_t<T, 4>(s, ab, v, o, st, per_sm);
+        case 5: return launch_mixed_blk_t<T, 5>(s, ab, v, o, st, per_sm);
+        case 6: return launch_mixed_blk_t<T, 6>(s, ab, v, o, st, per_sm);
+        case 7: return launch_mixed_blk_t<T, 7>(s, ab, v, o, st, per_sm);
+        case 8: return launch_mixed_blk_t<T, 8>(s, ab, v, o, st, per_sm);
+        case 9: return launch_mixed_blk_t<T, 9>(s, ab, v, o, st, per_sm);
+        default: return JCI_ERR_SPACE;
+    }
+}
+
 // Second kernel of the dense-product path.  The per-CTA scratch panels are
 // allocated on first use for the largest resident grid; `per_sm` picks the
 // CTAs per SM actually launched (0 = as many as fit), which trades latency
-// hiding against keeping the panels L2-resident.
+// hiding against keeping the panels L2-resident.  per_sm >= 16 selects the
+// column-blocked panel (k_sigma_mixed_blk) with per_sm - 16 CTAs per SM.
 template <typename T>
 static jci_status launch_mixed(jci_space *s, const FciArgs<T> &fa, const T *v, T *o,
                                cudaStream_t st, int per_sm) {
@@ -1004,6 +1194,7 @@ static jci_status launch_mixed(jci_space *s, const FciArgs<T> &fa, const T *v, T
     m.fsA = fa.fsA; m.fsB = fa.fsB; m.fpA = fa.fpA; m.fpB = fa.fpB;
     m.a1A = fa.a1A; m.m2 = fa.m2; m.occB = d->t[1].occ;
     m.skip = fa.skip;
+    if (per_sm >= 16) return launch_mixed_blk<T>(s, m, v, o, st, per_sm - 16);
     int TM = (m.mrows + 15) / 16;
     MixKernel<T> kern = mixed_kernel<T>(TM);
     if (!kern) return JCI_ERR_SPACE;
@@ -1095,9 +1286,9 @@ static bool ab_plan_possible(const FciTables *f, int tx, size_t w) {
 // Entry lists of the fused product with tx column threads, built on first use
 // (not while a stream is being captured).
 static jci_status ab_tables(jci_space *s, int tx, cudaStream_t st, AbTables **out) {
-    if (tx != 8 && tx != 16) return JCI_ERR_ARG;
+    if (tx != 8 && tx != 16 && tx != kMixBlock / 4) return JCI_ERR_ARG;
     FciTables *f = s->dev->fci;
-    AbTables &t = f->ab[tx == 16 ? 1 : 0];
+    AbTables &t = tx == kMixBlock / 4 ? f->abk : f->ab[tx == 16 ? 1 : 0];
     if (!t.ent) {
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         JCI_CUDA(cudaStreamIsCapturing(st, &cs));
@@ -1349,7 +1540,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     float bpanel = 1e30f, bmix2 = 1e30f, bab = 1e30f;
     int Rpanel = 1, Rmix2 = 1, txab = 0;
     if (mixed_possible(f, w))
-        for (int R : {1, 2, 4}) {
+        for (int R : {1, 2, 4, 16 + 1, 16 + 2, 16 + 4}) {  // whole-row panel, column-blocked
             float ms = timeit([&] { return launch_mixed<T>(s, ar, v, o, st, R); });
             if (ms < bpanel) { bpanel = ms; Rpanel = R; }
         }
@@ -1600,6 +1791,11 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, 
     }
     if (mode == 6 || mode == 7) {
         jci_status r = group_tables(s, s->dev->stream);
+        if (r) return r;
+    }
+    if ((mode == 1 || mode == 3 || mode == 6) && R >= 16) {  // column-blocked panel lists
+        AbTables *t = nullptr;
+        jci_status r = ab_tables(s, kMixBlock / 4, s->dev->stream, &t);
         if (r) return r;
     }
     f->tuned_mode[p] = mode;

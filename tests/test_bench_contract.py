@@ -7,8 +7,8 @@ import os
 import bench
 
 
-def _traffic(workload, mode, B):
-    p = bench.committed_profile(workload, mode, B)
+def _traffic(workload, mode, B, R=0):
+    p = bench.committed_profile(workload, mode, B, R)
     return p.get("dram_bytes_per_launch") if p else None
 
 
@@ -35,15 +35,19 @@ def test_every_traffic_entry_points_at_a_committed_summary():
         for key, plan in d["plans"].items():
             mode = int(key.split(":")[0])
             assert mode in bench.PLAN_NAMES
-            assert (":" in key) == (mode in (6, 7))   # group plans carry their variant
+            # group plans carry their variant, blocked panels a suffix
+            assert (":" in key.replace(":blk", "")) == (mode in (6, 7))
             assert plan["dram_bytes_per_launch"] > 0 and plan["kernels"]
             assert os.path.exists(os.path.join(bench.ROOT, plan["summary"]))
 
 
 def test_plan_description_names_each_plans_parameters():
     d = bench.sigma_plan_desc(7, 512, 16, 3)
-    assert d["beta_singles_threads"] == 512 and d["product_column_threads"] == 16
+    assert d["beta_singles_threads"] == 512 and d["product_engine"] == "16 column threads"
     assert "split over 4 warps, 2 column" in d["group_kernel"]
+    assert "tcgen05" in bench.sigma_plan_desc(7, 512, 64, 3)["product_engine"]
+    d = bench.sigma_plan_desc(6, 512, 18, 2)
+    assert d["product_ctas_per_sm"] == 2 and d["product_panel"] == "256-column blocks"
     assert "1 column" in bench.sigma_plan_desc(6, 256, 0, 1)["group_kernel"]
     assert "split over 4 warps, 1 column" in bench.sigma_plan_desc(6, 256, 0, 4)["group_kernel"]
     d = bench.sigma_plan_desc(3, 256, 0, 512)

@@ -130,7 +130,9 @@ def test_every_plan_at_fci12(prec):
     plans = [(0, 256, 4, 1), (1, 256, 0, 2), (2, 256, 0, 1), (3, 256, 0, 256),
              (4, 256, 16, 256), (5, 256, 16, 2), (5, 256, 8, 1), (6, 512, 0, 2),
              (7, 512, 16, 1), (7, 512, 16, 2), (7, 512, 16, 3), (7, 512, 16, 4),
-             (7, 512, 8, 3)]
+             (7, 512, 8, 3),
+             # the column-blocked panel (product CTAs per SM + 16)
+             (1, 256, 17, 2), (3, 256, 16, 256), (6, 512, 18, 2)]
     ran = 0
     for plan in plans:
         try:
@@ -140,7 +142,23 @@ def test_every_plan_at_fci12(prec):
         got = _gpu_sigma(s, v, prec)[rows].double().cpu().numpy()
         assert np.abs(got - ref).max() <= bar, (plan, np.abs(got - ref).max())
         ran += 1
-    assert ran >= 10
+    assert ran >= 13
+    s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [jb.FP64, jb.FP32])
+def test_blocked_panel_fci16(prec):
+    """FCI(16e,16o): the product through the column-blocked panel against the
+    pinned rows."""
+    import torch
+    s, g, _, _, _ = _space("fci16_16")
+    s.set_sigma_plan(prec, 6, 512, 18, 2)
+    v = hash_vector(s.ndets, int(g["sigma_seed"]))
+    got = _gpu_sigma(s, v, prec)[torch.from_numpy(g["rows"]).cuda()].double().cpu().numpy()
+    ref = g["sigma_rows"]
+    bar = (1e-12 if prec == jb.FP64 else 2e-6) * np.abs(ref).max()
+    assert np.abs(got - ref).max() <= bar
     s.close()
 
 
