@@ -573,7 +573,7 @@ def run_gpu(a):
             "kernel_ms_per_launch": avg_launch_s * 1e3,
             "model": "row-stream bytes B = 8 N (2 + s + d) per vector: each sigma row reads "
                      "its own C row and one C row per alpha single and double"}
-    for k in ("dram_gb_per_s", "l2_bytes_per_launch", "limiter", "summary"):
+    for k in ("dram_gb_per_s", "l2_bytes_per_launch", "dominant_kernel", "limiter", "summary"):
         if k in prof:
             roof[k] = prof[k]
     sp.close()

@@ -382,7 +382,10 @@ __global__ void __launch_bounds__(kMixThreads)
             }
             __syncthreads();
         }
-        // gather: every column of the row owned by one thread, fixed order
+        // gather: every column of the row owned by one thread, fixed order.
+        // The panel reads are random (DRAM once the panels outgrow L2); the
+        // singles loop takes its indices 8 at a time so that 8 panel reads
+        // are in flight per thread, and adds them in list order.
         const T *TU = Tb + (size_t)a.npair * a.nbp;
         T *srow = S + (long long)Ia * a.nb;
         for (int Ib = tid; Ib < a.nb; Ib += kMixThreads) {
@@ -393,7 +396,19 @@ __global__ void __launch_bounds__(kMixThreads)
                 oc &= oc - 1;
                 x += Tb[(size_t)(m * (m + 1) / 2 - 1) * a.nbp + Ib];
             }
-            for (int f = 0; f < a.sb; f++) {
+            int f = 0;
+            for (; f + 8 <= a.sb; f += 8) {
+                T t[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const long long o = (long long)(f + u) * a.nb + Ib;
+                    const uint32_t e = a.fsB[o];
+                    t[u] = flip(Tb[(size_t)a.fpB[o] * a.nbp + (e & 0x3fffffffu)], e >> 31);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u++) x += t[u];
+            }
+            for (; f < a.sb; f++) {
                 long long o = (long long)f * a.nb + Ib;
                 uint32_t e = a.fsB[o];
                 x += flip(Tb[(size_t)a.fpB[o] * a.nbp + (e & 0x3fffffffu)], e >> 31);

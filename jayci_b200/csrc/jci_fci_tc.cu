@@ -150,24 +150,6 @@ __device__ __forceinline__ void tc_fence_after() {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-// 32 consecutive accumulator columns of this thread's tensor-memory lane.
-__device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
-        "%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
-          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
-          "=r"(r[31])
-        : "r"(taddr)
-        : "memory");
-#pragma unroll
-    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
-}
-
 __device__ __forceinline__ void tc_wait_ld() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
@@ -250,28 +232,36 @@ __global__ void __launch_bounds__(NT, 1)
     bool failed = false;
 
     // Raw B chunk c into buffer b: rows Ja_j of C, the chunk's columns, as
-    // plain FP32 values at their places in the high-part tile (one 4-byte
-    // cp.async each: a core-matrix row holds 4 consecutive k of one column).
-    // Rows k >= K and columns past nb are zeros written directly.
+    // plain FP32 values at their places in the high-part tile.  A thread
+    // copies whole 16-byte pieces -- 4 consecutive k of one column, one
+    // 4-byte cp.async each (the 4 values come from 4 rows of C) -- and later
+    // splits exactly those pieces, so the split needs only its own copies
+    // (no barrier between copy and split).  Rows k >= K and columns past nb
+    // are zeros written directly.
     auto fetch_b = [&](int c, int b) {
         const int c0 = c * CW;
         const uint32_t bh = L.bh + (uint32_t)b * L.bstride;
-        for (int idx = tid; idx < CW * K8; idx += NT) {
-            const int n = idx % CW, k = idx / CW, col = c0 + n;
-            float *dst = reinterpret_cast<float *>(smem + bh + tc_off(n, k, K8));
-            if (k < K && col < nb)
-                __pipeline_memcpy_async(dst, V + (long long)jl[k] * nb + col, 4);
-            else
-                *dst = 0.f;
+        for (int idx = tid; idx < CW * (K8 / 4); idx += NT) {
+            const int n = idx % CW, kq = idx / CW, col = c0 + n;
+            float *dst = reinterpret_cast<float *>(smem + bh + tc_off(n, 4 * kq, K8));
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int k = 4 * kq + u;
+                if (k < K && col < nb)
+                    __pipeline_memcpy_async(dst + u, V + (long long)jl[k] * nb + col, 4);
+                else
+                    dst[u] = 0.f;
+            }
         }
         __pipeline_commit();
     };
-    // Split the landed raw chunk in buffer b in place: high part stays,
-    // remainder to the low-part tile.
+    // Split this thread's pieces of the landed raw chunk in buffer b in
+    // place: high part stays, remainder to the low-part tile.
     auto split_b = [&](int b) {
         const uint32_t bh = L.bh + (uint32_t)b * L.bstride, bl = L.bl + (uint32_t)b * L.bstride;
         for (int idx = tid; idx < CW * (K8 / 4); idx += NT) {
-            const uint32_t o = 16u * (uint32_t)idx;  // the tile is CW * K8 / 4 pieces of 16 bytes
+            const int n = idx % CW, kq = idx / CW;
+            const uint32_t o = tc_off(n, 4 * kq, K8);
             uint4 x = *reinterpret_cast<const uint4 *>(smem + bh + o);
             uint4 hi, lo;
             const uint32_t *xv = &x.x;
@@ -341,8 +331,7 @@ __global__ void __launch_bounds__(NT, 1)
         __syncthreads();  // jl before the B copies read it
         fetch_b(0, 0);
         if (a.nchunk > 1) fetch_b(1, 1);  // the previous string's MMAs are all done
-        __pipeline_wait_prior(a.nchunk > 1 ? 1 : 0);
-        __syncthreads();  // raw B(0) landed (every thread's copies)
+        __pipeline_wait_prior(a.nchunk > 1 ? 1 : 0);  // this thread's raw B(0) pieces
         split_b(0);
         fence_proxy_async();
         tc_fence_before();
@@ -357,13 +346,11 @@ __global__ void __launch_bounds__(NT, 1)
         for (int ci = 0; ci < a.nchunk; ci++) {
             const int b = ci & 1;
             const bool more = ci + 1 < a.nchunk;
-            __pipeline_wait_prior(0);  // this thread's raw B(ci+1) copies
-            tc_fence_before();
-            __syncthreads();  // raw B(ci+1) landed; gather(ci-1) and its T reads done
+            __pipeline_wait_prior(0);  // this thread's raw B(ci+1) pieces
             if (more) split_b(b ^ 1);
             fence_proxy_async();
             tc_fence_before();
-            __syncthreads();  // B(ci+1) split
+            __syncthreads();  // B(ci+1) split; gather(ci-1) and its T reads done
             if (tid == 0) {
                 // the chunk's entry lists, by bulk copy
                 const uint32_t e0 = a.base[ci], ne = a.base[ci + 1] - e0;
@@ -386,22 +373,28 @@ __global__ void __launch_bounds__(NT, 1)
             }
             tc_fence_after();
             if (ok && ci + 2 < a.nchunk) fetch_b(ci + 2, b);
-            const int wg = warp >> 2, row = 32 * (warp & 3) + lane;
-            if (ok && wg < MT) {
-                const int m = 128 * wg + row;
-#pragma unroll
-                for (int h = 0; h < CW / 32; h++) {
-                    float v[32];
-                    tc_ld32(tmem + ((uint32_t)(32 * (warp & 3)) << 16) +
-                                (uint32_t)((b * MT + wg) * CW + 32 * h),
-                            v);
+            // every warp moves one 8-column slice of one tile: (tile, slice)
+            // units of 128 lanes x 8 columns, warp quarter (warp & 3) -> lanes
+            const int row = 32 * (warp & 3) + lane;
+            if (ok) {
+                constexpr int NS = CW / 8;  // slices per tile
+                for (int u = warp >> 2; u < MT * NS; u += NT / 128) {
+                    const int t = u / NS, c8 = 8 * (u % NS), m = 128 * t + row;
+                    uint32_t r[8];
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]),
+                          "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                        : "r"(tmem + ((uint32_t)(32 * (warp & 3)) << 16) +
+                              (uint32_t)((b * MT + t) * CW + c8))
+                        : "memory");
                     tc_wait_ld();
                     if (m < a.mrows) {
-                        float4 *dst = reinterpret_cast<float4 *>(Ts + (size_t)m * CWP + 32 * h);
-#pragma unroll
-                        for (int q = 0; q < 8; q++)
-                            dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2],
-                                                 v[4 * q + 3]);
+                        float4 *dst = reinterpret_cast<float4 *>(Ts + (size_t)m * CWP + c8);
+                        dst[0] = make_float4(__uint_as_float(r[0]), __uint_as_float(r[1]),
+                                             __uint_as_float(r[2]), __uint_as_float(r[3]));
+                        dst[1] = make_float4(__uint_as_float(r[4]), __uint_as_float(r[5]),
+                                             __uint_as_float(r[6]), __uint_as_float(r[7]));
                     }
                 }
             }
