@@ -300,7 +300,11 @@ struct MixArgs {
     const int *skip;
 };
 
-template <typename T, int TM>
+// NB = 2: B chunks double-buffered (chunk c+1 copied while chunk c
+// multiplies); NB = 1: one buffer, so that two CTAs fit an SM where the
+// double-buffered form fits one (the other CTA's product then covers this
+// CTA's copies and gather).
+template <typename T, int TM, int NB = 2>
 __global__ void __launch_bounds__(kMixThreads)
     k_sigma_mixed(MixArgs<T> a, const T *__restrict__ V, T *__restrict__ S, T *__restrict__ Tbuf) {
     if (a.skip && *a.skip) return;
@@ -308,8 +312,8 @@ __global__ void __launch_bounds__(kMixThreads)
     constexpr int MP = 16 * TM;
     const int K = a.sa;
     T *As = reinterpret_cast<T *>(smem_raw);          // [K][MP]
-    T *Bs = As + (size_t)K * MP;                      // [2][K][64]
-    int *jl = reinterpret_cast<int *>(Bs + 2 * (size_t)K * kMixCols);  // [K]
+    T *Bs = As + (size_t)K * MP;                      // [NB][K][64]
+    int *jl = reinterpret_cast<int *>(Bs + NB * (size_t)K * kMixCols);  // [K]
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     T *Tb = Tbuf + (size_t)blockIdx.x * a.mrows * a.nbp;
     const int nchunk = a.nbp / kMixCols;
@@ -342,8 +346,8 @@ __global__ void __launch_bounds__(kMixThreads)
         stage(0, Bs);
         for (int ci = 0; ci < nchunk; ci++) {
             const int c0 = ci * kMixCols;
-            T *Bc = Bs + (size_t)(ci & 1) * K * kMixCols;
-            if (ci + 1 < nchunk) {
+            T *Bc = Bs + (size_t)(NB == 2 ? (ci & 1) : 0) * K * kMixCols;
+            if (NB == 2 && ci + 1 < nchunk) {
                 stage(ci + 1, Bs + (size_t)((ci + 1) & 1) * K * kMixCols);
                 __pipeline_wait_prior(1);
             } else {
@@ -381,6 +385,7 @@ __global__ void __launch_bounds__(kMixThreads)
                 }
             }
             __syncthreads();
+            if (NB == 1 && ci + 1 < nchunk) stage(ci + 1, Bs);
         }
         // gather: every column of the row owned by one thread, fixed order.
         // The panel reads are random (DRAM once the panels outgrow L2); the
@@ -968,8 +973,8 @@ static size_t rows_smem(int nb, int npair, int da, int RB, size_t w) {
     return (size_t)RB * nb * w + (size_t)RB * npair * w + (size_t)RB * da * (w + 4) + 16;
 }
 
-static size_t mix_smem(int K, int TM, size_t w) {
-    return (size_t)K * 16 * TM * w + 2 * (size_t)K * kMixCols * w + (size_t)K * 4 + 16;
+static size_t mix_smem(int K, int TM, size_t w, int nb = 2) {
+    return (size_t)K * 16 * TM * w + (size_t)nb * K * kMixCols * w + (size_t)K * 4 + 16;
 }
 
 static size_t fci_smem(int nb, int npair, int R, size_t w) {
@@ -1130,6 +1135,22 @@ static MixKernel<T> mixed_kernel(int TM) {
     }
 }
 
+template <typename T>
+static MixKernel<T> mixed_kernel1(int TM) {
+    switch (TM) {
+        case 1: return k_sigma_mixed<T, 1, 1>;
+        case 2: return k_sigma_mixed<T, 2, 1>;
+        case 3: return k_sigma_mixed<T, 3, 1>;
+        case 4: return k_sigma_mixed<T, 4, 1>;
+        case 5: return k_sigma_mixed<T, 5, 1>;
+        case 6: return k_sigma_mixed<T, 6, 1>;
+        case 7: return k_sigma_mixed<T, 7, 1>;
+        case 8: return k_sigma_mixed<T, 8, 1>;
+        case 9: return k_sigma_mixed<T, 9, 1>;
+        default: return nullptr;
+    }
+}
+
 static bool mixed_possible(const FciTables *f, size_t w) {
     int mrows = f->npair + 1, TM = (mrows + 15) / 16;
     return TM <= 9 && f->sa >= 1 && mix_smem(f->sa, TM, w) <= f->smem_max;
@@ -1211,10 +1232,21 @@ static jci_status launch_mixed(jci_space *s, const FciArgs<T> &fa, const T *v, T
     m.skip = fa.skip;
     if (per_sm >= 16) return launch_mixed_blk<T>(s, m, v, o, st, per_sm - 16);
     int TM = (m.mrows + 15) / 16;
-    MixKernel<T> kern = mixed_kernel<T>(TM);
-    if (!kern) return JCI_ERR_SPACE;
-    size_t smem = mix_smem(m.sa, TM, sizeof(T));
+    MixKernel<T> kern = mixed_kernel<T>(TM), kern1 = mixed_kernel1<T>(TM);
+    if (!kern || !kern1) return JCI_ERR_SPACE;
+    size_t smem = mix_smem(m.sa, TM, sizeof(T)), smem1 = mix_smem(m.sa, TM, sizeof(T), 1);
     JCI_CUDA(smem_optin(kern));
+    JCI_CUDA(smem_optin(kern1));
+    {
+        // one B buffer when that lets a second CTA share each SM
+        int occ2 = 0, occ1 = 0;
+        JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, kern, kMixThreads, smem));
+        JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, kern1, kMixThreads, smem1));
+        if (occ2 < 2 && occ1 > occ2) {
+            kern = kern1;
+            smem = smem1;
+        }
+    }
     if (!f->mix_grid[prec]) {
         int occ = 0, nsm = 0;
         JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kMixThreads, smem));
