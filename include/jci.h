@@ -207,7 +207,9 @@ jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sigma,
  * 3-4: of the alpha pass; modes 6-7: of the beta-singles stream), `rows`
  * (mode 0: alpha rows staged per pass; modes 1-3 and 6: product CTAs per
  * SM, 0 = as many as fit, plus 16 for the panel cut into 256-column blocks
- * gathered block by block (modes 1, 3, 6); modes 4, 5, 7: column threads of the fused
+ * gathered block by block, plus 32 for one panel per alpha row built and
+ * gathered by all CTAs from a shared work queue (modes 1, 3, 6); modes 4,
+ * 5, 7: column threads of the fused
  * product, 8 (CUDA cores, 32-column chunks) or 16 (tensor cores, 64-column
  * chunks: FP64 mma.sync in FP64, 3xTF32 in FP32), or in FP32 32 / 64 (the
  * tcgen05 engine, 32- / 64-column chunks)), `batch` (modes 1, 2, 5: alpha strings per CTA of the

@@ -121,6 +121,7 @@ jci_status jci_sigma(jci_space *s, int nvec, const double *v, double *sig, int p
         if (cudaMemcpyAsync(dst, d->io_s, bytes, cudaMemcpyDeviceToHost, st)) r = JCI_ERR_CUDA;
     }
     if (!r && cudaStreamSynchronize(st) != cudaSuccess) r = JCI_ERR_CUDA;
+    if (!r) r = fci_wait_status(s);
     if (!r && precision == JCI_FP32)
         for (size_t i = 0; i < tmp.size(); i++) sig[i] = tmp[i];
     return r;

@@ -211,6 +211,77 @@ __global__ void __launch_bounds__(256)
         partial[(long long)blockIdx.x * kGramRows * kGramCols + e] = red[e / p][e % p];
 }
 
+// G = X^T y for one vector y (p = 1: the basis products of every iteration)
+// on the FP64 FMA pipes: an m8n8k4 product with one valid column would do
+// eight times the arithmetic, and at 48 rows that padding costs as much time
+// as the loads.  Row i belongs to warp i % 8; every warp reads the whole
+// slice of y (from L1 after the first warp) and of its rows, lane l taking
+// the element pairs lo + 64 j + 2 l in ascending j, U pairs per step, so a
+// thread keeps MT x U 16-byte loads in flight.  A row's sum runs in the same
+// order whatever MT and U, so host-driven and graph-captured iterations
+// (different MT) agree bitwise.  Block partial of row i in partial[blk][i],
+// summed in block order by k_gram_finish.
+template <int MT>
+__global__ void __launch_bounds__(256)
+    k_gram_vec(const double *__restrict__ X, int m, const double *__restrict__ y, long long ld,
+               long long n, long long chunk, double *__restrict__ partial, GramDev gd) {
+    if (gd.stop && *gd.stop) return;
+    if (gd.mdev) m = *gd.mdev + gd.madd;
+    constexpr int U = MT <= 2 ? 8 : (MT <= 4 ? 4 : 2);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long lo = (long long)blockIdx.x * chunk, hi = min(n, lo + chunk);
+    const double *xr[MT];
+    bool xv[MT];
+#pragma unroll
+    for (int a = 0; a < MT; a++) {
+        xv[a] = 8 * a + warp < m;
+        xr[a] = X + (long long)(xv[a] ? 8 * a + warp : 0) * ld;
+    }
+    double acc[MT];
+#pragma unroll
+    for (int a = 0; a < MT; a++) acc[a] = 0.0;
+    for (long long k0 = lo + 2 * lane; k0 < hi; k0 += 64 * U) {
+        double2 yv[U], xvv[U][MT];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const long long k = k0 + 64 * u;
+            yv[u] = load_pair(y, k, hi, true);
+#pragma unroll
+            for (int a = 0; a < MT; a++) xvv[u][a] = load_pair(xr[a], k, hi, xv[a]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+#pragma unroll
+            for (int a = 0; a < MT; a++) {
+                acc[a] = fma(xvv[u][a].x, yv[u].x, acc[a]);
+                acc[a] = fma(xvv[u][a].y, yv[u].y, acc[a]);
+            }
+    }
+#pragma unroll
+    for (int a = 0; a < MT; a++) {
+        double s = acc[a];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0 && xv[a])
+            partial[(long long)blockIdx.x * kGramRows * kGramCols + 8 * a + warp] = s;
+    }
+}
+
+using GramVecKernel = void (*)(const double *, int, const double *, long long, long long,
+                               long long, double *, GramDev);
+
+static GramVecKernel gram_vec_kernel(int mt) {
+    switch (mt) {
+        case 1: return k_gram_vec<1>;
+        case 2: return k_gram_vec<2>;
+        case 3: return k_gram_vec<3>;
+        case 4: return k_gram_vec<4>;
+        case 5: return k_gram_vec<5>;
+        case 6: return k_gram_vec<6>;
+        case 7: return k_gram_vec<7>;
+        default: return k_gram_vec<8>;
+    }
+}
+
 // Single dot product x . y (norms): every lane loads, block partial in
 // partial[blk][0], summed in block order by k_gram_finish.
 __global__ void __launch_bounds__(256)
@@ -325,7 +396,7 @@ __global__ void k_orth_update(double *__restrict__ t, long long n, long long ld,
          k2 += (long long)gridDim.x * blockDim.x) {
         const long long k = 2 * k2;
         double2 s = *reinterpret_cast<const double2 *>(t + k);
-#pragma unroll 4
+#pragma unroll 8
         for (int i = 0; i < m; i++) {
             const double2 x = *reinterpret_cast<const double2 *>(X + i * ld + k);
             s.x -= c[i] * x.x;
@@ -735,6 +806,9 @@ static jci_status gram(Ctx &c, const double *X, int m, const double *Y, int p, d
     int nb = (int)((c.n + chunk - 1) / chunk);
     if (dot)
         k_dot<<<nb, 256, 0, c.st>>>(X, Y, c.n, chunk, c.b->partial, gd);
+    else if (p == 1)
+        gram_vec_kernel((m + 7) / 8)<<<nb, 256, 0, c.st>>>(X, m, Y, c.ld, c.n, chunk,
+                                                            c.b->partial, gd);
     else
         gram_kernel((m + 7) / 8, (p + 7) / 8)<<<nb, 256, 0, c.st>>>(X, m, Y, p, c.ld, c.n,
                                                                      chunk, c.b->partial, gd);
@@ -1072,6 +1146,7 @@ static jci_status graph_iterations(Ctx &c, const jci_davidson_opts *o, bool fp32
     JCI_CUDA(cudaMemcpyAsync(G.data(), b->G, kMaxKry * kMaxKry * sizeof(double),
                              cudaMemcpyDeviceToHost, c.st));
     JCI_CUDA(cudaStreamSynchronize(c.st));
+    if ((r = fci_wait_status(c.s))) return r;
     const int nh = std::min(h.nhist, kHist);
     for (int i = 0; i < nh; i++) {
         rnorm = hist[i].rnorm;
@@ -1354,6 +1429,8 @@ jci_status davidson(jci_space *s, const jci_davidson_opts *o, double *energies, 
             r = run_sequential(c, o, mixed, w, Y, ckdim, citer, conv, rnorm);
     }
     if (r) return r;
+    // a product kernel that gave up a bounded wait left its sigma incomplete
+    if ((r = fci_wait_status(s))) return r;
     double core = s->nucrep + s->frzcore;
     for (int k = 0; k < o->nroots; k++) energies[k] = w[k] + core;
     std::vector<double> host;

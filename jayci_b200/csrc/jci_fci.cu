@@ -57,16 +57,29 @@ struct FciTables {
     uint32_t *sortB = nullptr;     // [Ib][f] beta singles sorted by target
     AbTables ab[2];                // fused product's entry lists, 8 / 16 column threads
     GroupTables grp[2];            // same-spin doubles by string groups, per spin
-    int *tc_status = nullptr;      // set by the tcgen05 product if a bounded wait expired
+    int *tc_status = nullptr;      // set by a product kernel whose bounded wait expired
+                                   // (tcgen05 product, row-shared panels)
     AbTables abk;                  // per-block lists of the column-blocked panel product
     void *tbufk[2] = {nullptr, nullptr};  // its per-CTA scratch blocks
     int mixk_grid[2] = {0, 0};
+    void *wbuf[2] = {nullptr, nullptr};   // row-shared panels of the queued product
+    void *wctl[2] = {nullptr, nullptr};   // and its queue counters (WaveCtl)
 };
 
 bool fci_supported(const jci_space *s) {
     const DeviceState *d = s->dev;
     if (!d || !d->single_group || !d->fci) return false;
     return d->fci->smem_max > 0;
+}
+
+jci_status fci_wait_status(jci_space *s) {
+    const DeviceState *d = s->dev;
+    if (!d || !d->fci || !d->fci->tc_status) return JCI_OK;
+    int flag = 0;
+    JCI_CUDA(cudaMemcpy(&flag, d->fci->tc_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!flag) return JCI_OK;
+    JCI_CUDA(cudaMemset(d->fci->tc_status, 0, sizeof(int)));
+    return JCI_ERR_TIMEOUT;
 }
 
 void fci_free(DeviceState *d) {
@@ -83,6 +96,10 @@ void fci_free(DeviceState *d) {
     cudaFree(f->tc_status);
     cudaFree(f->tbufk[0]);
     cudaFree(f->tbufk[1]);
+    for (int p = 0; p < 2; p++) {
+        cudaFree(f->wbuf[p]);
+        cudaFree(f->wctl[p]);
+    }
     ab_tables_free(&f->abk);
     ab_tables_free(&f->ab[0]);
     ab_tables_free(&f->ab[1]);
@@ -545,6 +562,222 @@ __global__ void __launch_bounds__(kMixThreads)
                 }
             }
             __syncthreads();
+        }
+    }
+}
+
+// ---- dense product through row panels shared by all CTAs -------------------
+//
+// The product of k_sigma_mixed with each alpha string's panel T (mrows x nbp)
+// built by many CTAs at once and kept in L2, instead of one private panel
+// per CTA (296 panels of 14 MB at FCI(16,16): written to and gathered back
+// from DRAM at random).  The work is a queue of items claimed with one
+// atomic counter:
+//   step i:  the GEMM items of row i (kWaveChunks 64-column chunks of T each),
+//            then the gather items of row i - kWaveLag (kMixThreads beta
+//            strings each: the same sums as k_sigma_mixed's gather);
+// row i's panel is buffer i % kWaveBufs.  A gather item waits until all GEMM
+// items of its row are done; a GEMM item waits until all gather items of
+// the row that used its buffer before are done.  Every wait is on an item
+// that was claimed earlier (kWaveBufs > kWaveLag), by a CTA that is running,
+// so the queue cannot stall on residency; waits are bounded (one second of
+// global time), after which the kernel sets *status and returns.  Each T
+// element and each sigma element is computed by one item in the order of
+// k_sigma_mixed: the result is bitwise that of k_sigma_mixed.
+constexpr int kWaveBufs = 4, kWaveLag = 2, kWaveChunks = 4;
+
+struct WaveCtl {
+    int next;                    // next item to claim
+    int err;                     // a bounded wait expired
+    int gemm_done[kWaveBufs];    // GEMM items finished per buffer (cumulative)
+    int gather_done[kWaveBufs];  // gather items finished per buffer (cumulative)
+};
+
+__device__ __forceinline__ uint64_t wave_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Thread 0: wait until *cnt >= target; false after about one second or when
+// another CTA has given up (ctl->err).
+__device__ __forceinline__ bool wave_wait(const int *cnt, int target, WaveCtl *ctl) {
+    const uint64_t t0 = wave_ns();
+    for (long long it = 0;; it++) {
+        int v;
+        asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(cnt) : "memory");
+        if (v >= target) return true;
+        if ((it & 63) == 63) {
+            if (*(volatile int *)&ctl->err) return false;
+            if (wave_ns() - t0 > 1000000000ull || it > (1ll << 28)) return false;
+        }
+        __nanosleep(64);
+    }
+}
+
+template <typename T, int TM, int NB>
+__global__ void __launch_bounds__(kMixThreads)
+    k_sigma_wave(MixArgs<T> a, const T *__restrict__ V, T *__restrict__ S, T *__restrict__ Tw,
+                 WaveCtl *ctl, int ngi, int nhi, int *status) {
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_item, s_ok;
+    constexpr int MP = 16 * TM;
+    const int K = a.sa;
+    T *As = reinterpret_cast<T *>(smem_raw);          // [K][MP]
+    T *Bs = As + (size_t)K * MP;                      // [NB][K][64]
+    int *jl = reinterpret_cast<int *>(Bs + NB * (size_t)K * kMixCols);  // [K]
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int nchunk = a.nbp / kMixCols;
+    const size_t panel = (size_t)a.mrows * a.nbp;
+    const int lag = min(kWaveLag, a.na), per = ngi + nhi;
+    const long long pre = (long long)lag * ngi, mid = (long long)(a.na - lag) * per;
+    const long long total = (long long)a.na * per;
+    auto stage = [&](int c, T *buf) {
+        const int c0 = c * kMixCols;
+        for (int idx = tid; idx < K * kMixCols; idx += kMixThreads) {
+            int j = idx >> 6, col = c0 + (idx & 63);
+            if (col < a.nb)
+                __pipeline_memcpy_async(buf + idx, V + (long long)jl[j] * a.nb + col, sizeof(T));
+            else
+                buf[idx] = T(0);
+        }
+        __pipeline_commit();
+    };
+    for (;;) {
+        __syncthreads();  // the previous item is done with shared memory
+        if (tid == 0) s_item = atomicAdd(&ctl->next, 1);
+        __syncthreads();
+        const long long q = s_item;
+        if (q >= total) return;
+        int row, sub;
+        bool gemm;
+        if (q < pre) {
+            row = (int)(q / ngi); sub = (int)(q % ngi); gemm = true;
+        } else if (q - pre < mid) {
+            const long long r = q - pre;
+            const int step = lag + (int)(r / per), k = (int)(r % per);
+            gemm = k < ngi;
+            row = gemm ? step : step - lag;
+            sub = gemm ? k : k - ngi;
+        } else {
+            const long long r = q - pre - mid;
+            row = a.na - lag + (int)(r / nhi); sub = (int)(r % nhi); gemm = false;
+        }
+        const int buf = row % kWaveBufs, gen = row / kWaveBufs;
+        T *Tb = Tw + (size_t)buf * panel;
+        if (tid == 0) {
+            bool ok = gemm ? (gen == 0 || wave_wait(&ctl->gather_done[buf], gen * nhi, ctl))
+                           : wave_wait(&ctl->gemm_done[buf], (gen + 1) * ngi, ctl);
+            if (!ok) {
+                atomicExch(&ctl->err, 1);
+                if (status) atomicExch(status, 1);
+            }
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) return;
+        if (gemm) {
+            const int Ia = row;
+            for (int idx = tid; idx < K * MP; idx += kMixThreads) {
+                int j = idx / MP, m = idx - j * MP;
+                long long o = (long long)j * a.na + Ia;
+                uint32_t e = a.fsA[o];
+                T v = T(0);
+                if (m < a.npair) v = a.m2[eri_index(a.fpA[o], m)];
+                else if (m == a.npair) v = a.a1A[o];
+                As[idx] = flip(v, e >> 31);
+                if (m == 0) jl[j] = (int)(e & 0x3fffffffu);
+            }
+            __syncthreads();
+            const int c_lo = sub * kWaveChunks, c_hi = min(nchunk, c_lo + kWaveChunks);
+            stage(c_lo, Bs);
+            for (int ci = c_lo; ci < c_hi; ci++) {
+                const int c0 = ci * kMixCols;
+                T *Bc = Bs + (size_t)(NB == 2 ? ((ci - c_lo) & 1) : 0) * K * kMixCols;
+                if (NB == 2 && ci + 1 < c_hi) {
+                    stage(ci + 1, Bs + (size_t)((ci + 1 - c_lo) & 1) * K * kMixCols);
+                    __pipeline_wait_prior(1);
+                } else {
+                    __pipeline_wait_prior(0);
+                }
+                __syncthreads();
+                T acc[TM][4];
+#pragma unroll
+                for (int i = 0; i < TM; i++)
+#pragma unroll
+                    for (int qq = 0; qq < 4; qq++) acc[i][qq] = T(0);
+#pragma unroll 4
+                for (int k = 0; k < K; k++) {
+                    const T *br = Bc + k * kMixCols + tx;
+                    T b0 = br[0], b1 = br[16], b2 = br[32], b3 = br[48];
+                    const T *ar = As + k * MP + ty * TM;
+#pragma unroll
+                    for (int i = 0; i < TM; i++) {
+                        T av = ar[i];
+                        acc[i][0] = fma(av, b0, acc[i][0]);
+                        acc[i][1] = fma(av, b1, acc[i][1]);
+                        acc[i][2] = fma(av, b2, acc[i][2]);
+                        acc[i][3] = fma(av, b3, acc[i][3]);
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < TM; i++) {
+                    int m = ty * TM + i;
+                    if (m < a.mrows) {
+                        T *dst = Tb + (size_t)m * a.nbp + c0 + tx;
+#pragma unroll
+                        for (int qq = 0; qq < 4; qq++) dst[16 * qq] = acc[i][qq];
+                    }
+                }
+                __syncthreads();
+                if (NB == 1 && ci + 1 < c_hi) stage(ci + 1, Bs);
+            }
+            // release (the pattern of a grid barrier): the CTA's panel stores,
+            // then one thread's fence and count
+            __syncthreads();
+            if (tid == 0) {
+                __threadfence();
+                atomicAdd(&ctl->gemm_done[buf], 1);
+            }
+        } else {
+            const int Ia = row, Ib = sub * kMixThreads + tid;
+            if (Ib < a.nb) {
+                // panel reads from L2 (__ldcg): the buffer was rewritten by
+                // other SMs since this SM last read it
+                const T *TU = Tb + (size_t)a.npair * a.nbp;
+                T x = __ldcg(TU + Ib);
+                uint64_t oc = a.occB[Ib];
+                while (oc) {
+                    int m = __ffsll((long long)oc);
+                    oc &= oc - 1;
+                    x += __ldcg(Tb + (size_t)(m * (m + 1) / 2 - 1) * a.nbp + Ib);
+                }
+                int f = 0;
+                for (; f + 8 <= a.sb; f += 8) {
+                    T t[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        const long long o = (long long)(f + u) * a.nb + Ib;
+                        const uint32_t e = a.fsB[o];
+                        t[u] = flip(__ldcg(Tb + (size_t)a.fpB[o] * a.nbp + (e & 0x3fffffffu)),
+                                    e >> 31);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; u++) x += t[u];
+                }
+                for (; f < a.sb; f++) {
+                    long long o = (long long)f * a.nb + Ib;
+                    uint32_t e = a.fsB[o];
+                    x += flip(__ldcg(Tb + (size_t)a.fpB[o] * a.nbp + (e & 0x3fffffffu)), e >> 31);
+                }
+                S[(long long)Ia * a.nb + Ib] += x;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                __threadfence();
+                atomicAdd(&ctl->gather_done[buf], 1);
+            }
         }
     }
 }
@@ -1213,11 +1446,72 @@ static jci_status launch_mixed_blk(jci_space *s, const MixArgs<T> &m, const T *v
     }
 }
 
+template <typename T>
+using WaveKernel = void (*)(MixArgs<T>, const T *, T *, T *, WaveCtl *, int, int, int *);
+
+template <typename T, int NB>
+static WaveKernel<T> wave_kernel(int TM) {
+    switch (TM) {
+        case 1: return k_sigma_wave<T, 1, NB>;
+        case 2: return k_sigma_wave<T, 2, NB>;
+        case 3: return k_sigma_wave<T, 3, NB>;
+        case 4: return k_sigma_wave<T, 4, NB>;
+        case 5: return k_sigma_wave<T, 5, NB>;
+        case 6: return k_sigma_wave<T, 6, NB>;
+        case 7: return k_sigma_wave<T, 7, NB>;
+        case 8: return k_sigma_wave<T, 8, NB>;
+        case 9: return k_sigma_wave<T, 9, NB>;
+        default: return nullptr;
+    }
+}
+
+// The product through row panels shared by all CTAs (k_sigma_wave) with
+// per_sm CTAs per SM (0 = as many as fit).  The kWaveBufs panels and the
+// queue counters are allocated on first use; the counters are cleared on
+// the stream before every launch.
+template <typename T>
+static jci_status launch_wave(jci_space *s, const MixArgs<T> &m, const T *v, T *o,
+                              cudaStream_t st, int per_sm) {
+    DeviceState *d = s->dev;
+    FciTables *f = d->fci;
+    const int prec = sizeof(T) == 8 ? 0 : 1;
+    const int TM = (m.mrows + 15) / 16;
+    WaveKernel<T> kern = wave_kernel<T, 2>(TM), kern1 = wave_kernel<T, 1>(TM);
+    if (!kern || !kern1) return JCI_ERR_SPACE;
+    size_t smem = mix_smem(m.sa, TM, sizeof(T)), smem1 = mix_smem(m.sa, TM, sizeof(T), 1);
+    JCI_CUDA(smem_optin(kern));
+    JCI_CUDA(smem_optin(kern1));
+    int occ = 0, occ1 = 0, nsm = 0;
+    JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kMixThreads, smem));
+    JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, kern1, kMixThreads, smem1));
+    JCI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d->device));
+    if (occ < 2 && occ1 > occ) {  // one B buffer when that lets a second CTA share each SM
+        kern = kern1;
+        smem = smem1;
+        occ = occ1;
+    }
+    if (occ < 1) return JCI_ERR_SPACE;
+    const int nchunk = m.nbp / kMixCols;
+    const int ngi = (nchunk + kWaveChunks - 1) / kWaveChunks;
+    const int nhi = (m.nb + kMixThreads - 1) / kMixThreads;
+    int grid = nsm * (per_sm > 0 && per_sm < occ ? per_sm : occ);
+    if ((long long)m.na * (ngi + nhi) + grid >= (1ll << 31)) return JCI_ERR_SPACE;
+    if (!f->wbuf[prec]) {
+        JCI_CUDA(cudaMalloc(&f->wbuf[prec], (size_t)kWaveBufs * m.mrows * m.nbp * sizeof(T)));
+        JCI_CUDA(cudaMalloc(&f->wctl[prec], sizeof(WaveCtl)));
+    }
+    JCI_CUDA(cudaMemsetAsync(f->wctl[prec], 0, sizeof(WaveCtl), st));
+    kern<<<grid, kMixThreads, smem, st>>>(m, v, o, (T *)f->wbuf[prec], (WaveCtl *)f->wctl[prec],
+                                          ngi, nhi, f->tc_status);
+    return JCI_OK;
+}
+
 // Second kernel of the dense-product path.  The per-CTA scratch panels are
 // allocated on first use for the largest resident grid; `per_sm` picks the
 // CTAs per SM actually launched (0 = as many as fit), which trades latency
 // hiding against keeping the panels L2-resident.  per_sm >= 16 selects the
-// column-blocked panel (k_sigma_mixed_blk) with per_sm - 16 CTAs per SM.
+// column-blocked panel (k_sigma_mixed_blk) with per_sm - 16 CTAs per SM,
+// per_sm >= 32 the row-shared panels (k_sigma_wave) with per_sm - 32.
 template <typename T>
 static jci_status launch_mixed(jci_space *s, const FciArgs<T> &fa, const T *v, T *o,
                                cudaStream_t st, int per_sm) {
@@ -1230,6 +1524,7 @@ static jci_status launch_mixed(jci_space *s, const FciArgs<T> &fa, const T *v, T
     m.fsA = fa.fsA; m.fsB = fa.fsB; m.fpA = fa.fpA; m.fpB = fa.fpB;
     m.a1A = fa.a1A; m.m2 = fa.m2; m.occB = d->t[1].occ;
     m.skip = fa.skip;
+    if (per_sm >= 32) return launch_wave<T>(s, m, v, o, st, per_sm - 32);
     if (per_sm >= 16) return launch_mixed_blk<T>(s, m, v, o, st, per_sm - 16);
     int TM = (m.mrows + 15) / 16;
     MixKernel<T> kern = mixed_kernel<T>(TM), kern1 = mixed_kernel1<T>(TM);
@@ -1587,7 +1882,8 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     float bpanel = 1e30f, bmix2 = 1e30f, bab = 1e30f;
     int Rpanel = 1, Rmix2 = 1, txab = 0;
     if (mixed_possible(f, w))
-        for (int R : {1, 2, 4, 16 + 1, 16 + 2, 16 + 4}) {  // whole-row panel, column-blocked
+        // whole-row panel per CTA, column-blocked, row panels shared by all CTAs
+        for (int R : {1, 2, 4, 16 + 1, 16 + 2, 16 + 4}) {
             float ms = timeit([&] { return launch_mixed<T>(s, ar, v, o, st, R); });
             if (ms < bpanel) { bpanel = ms; Rpanel = R; }
         }
@@ -1840,7 +2136,7 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, 
         jci_status r = group_tables(s, s->dev->stream);
         if (r) return r;
     }
-    if ((mode == 1 || mode == 3 || mode == 6) && R >= 16) {  // column-blocked panel lists
+    if ((mode == 1 || mode == 3 || mode == 6) && R >= 16 && R < 32) {  // column-blocked lists
         AbTables *t = nullptr;
         jci_status r = ab_tables(s, kMixBlock / 4, s->dev->stream, &t);
         if (r) return r;

@@ -9,6 +9,9 @@ namespace jci {
 
 // FCI / CAS fast path (single electron-occupation group per spin), jci_fci.cu.
 bool fci_supported(const jci_space *s);
+// JCI_ERR_TIMEOUT (and the flag cleared) if a product kernel's bounded
+// device wait expired since the last call; synchronises with the device.
+jci_status fci_wait_status(jci_space *s);
 jci_status fci_prepare(jci_space *s);
 jci_status fci_sigma(jci_space *s, int nvec, const void *v, void *sig, long long ld,
                      int precision, cudaStream_t st);

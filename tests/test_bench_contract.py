@@ -35,8 +35,8 @@ def test_every_traffic_entry_points_at_a_committed_summary():
         for key, plan in d["plans"].items():
             mode = int(key.split(":")[0])
             assert mode in bench.PLAN_NAMES
-            # group plans carry their variant, blocked panels a suffix
-            assert (":" in key.replace(":blk", "")) == (mode in (6, 7))
+            # group plans carry their variant, blocked and shared panels a suffix
+            assert (":" in key.replace(":blk", "").replace(":row", "")) == (mode in (6, 7))
             assert plan["dram_bytes_per_launch"] > 0 and plan["kernels"]
             assert os.path.exists(os.path.join(bench.ROOT, plan["summary"]))
 
@@ -48,6 +48,9 @@ def test_plan_description_names_each_plans_parameters():
     assert "tcgen05" in bench.sigma_plan_desc(7, 512, 64, 3)["product_engine"]
     d = bench.sigma_plan_desc(6, 512, 18, 2)
     assert d["product_ctas_per_sm"] == 2 and d["product_panel"] == "256-column blocks"
+    d = bench.sigma_plan_desc(6, 512, 33, 2)
+    assert d["product_ctas_per_sm"] == 1 and "shared by all CTAs" in d["product_panel"]
+    assert bench.sigma_plan_desc(6, 512, 2, 2)["product_panel"] == "whole alpha row per CTA"
     assert "1 column" in bench.sigma_plan_desc(6, 256, 0, 1)["group_kernel"]
     assert "split over 4 warps, 1 column" in bench.sigma_plan_desc(6, 256, 0, 4)["group_kernel"]
     d = bench.sigma_plan_desc(3, 256, 0, 512)
