@@ -231,6 +231,16 @@ jci_status jci_sigma_tuning(const jci_space *s, int precision, int *mode,
 jci_status jci_sigma_set_plan(jci_space *s, int precision, int mode,
                               int threads, int rows, int batch);
 
+/* Test hook for the device-side wait bounds.  The next sigma whose product
+ * runs through the row panels shared by all CTAs (plan rows >= 32) leaves
+ * the panel work of its first two alpha rows undone, so the gathers that
+ * depend on it wait until their bound (about one second) expires; that
+ * sigma's output is then incomplete and the next host-synchronising call
+ * (jci_sigma, jci_davidson) returns JCI_ERR_TIMEOUT, after which the space
+ * works as before.  JCI_ERR_STATE for a space without device tables.  No
+ * reference counterpart. */
+jci_status jci_test_expire_next_wait(jci_space *s);
+
 typedef struct {
         int maxiter;      /* &dalginfo defaults: 20 */
         int krymin;       /* 3 */

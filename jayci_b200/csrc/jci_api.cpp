@@ -152,6 +152,12 @@ jci_status jci_sigma_set_plan(jci_space *s, int precision, int mode, int threads
     return fci_force_plan(s, precision, mode, threads, rows, batch);
 }
 
+jci_status jci_test_expire_next_wait(jci_space *s) {
+    if (!s) return JCI_ERR_ARG;
+    if (!s->have_ints || !fci_supported(s)) return JCI_ERR_STATE;
+    return fci_arm_wait_expiry(s);
+}
+
 void jci_davidson_defaults(jci_davidson_opts *o) {
     if (!o) return;
     memset(o, 0, sizeof(*o));

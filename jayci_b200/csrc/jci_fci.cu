@@ -64,12 +64,19 @@ struct FciTables {
     int mixk_grid[2] = {0, 0};
     void *wbuf[2] = {nullptr, nullptr};   // row-shared panels of the queued product
     void *wctl[2] = {nullptr, nullptr};   // and its queue counters (WaveCtl)
+    int wave_expire = 0;           // test hook: the next such launch skips work (see below)
 };
 
 bool fci_supported(const jci_space *s) {
     const DeviceState *d = s->dev;
     if (!d || !d->single_group || !d->fci) return false;
     return d->fci->smem_max > 0;
+}
+
+jci_status fci_arm_wait_expiry(jci_space *s) {
+    if (!s->dev || !s->dev->fci) return JCI_ERR_STATE;
+    s->dev->fci->wave_expire = 1;
+    return JCI_OK;
 }
 
 jci_status fci_wait_status(jci_space *s) {
@@ -1446,6 +1453,11 @@ static jci_status launch_mixed_blk(jci_space *s, const MixArgs<T> &m, const T *v
     }
 }
 
+// Test hook: start the queue past the GEMM items of the first kWaveLag rows,
+// so that nothing ever completes them and the gathers of those rows wait
+// until their bounded waits expire.
+__global__ void k_wave_arm(WaveCtl *ctl, int first) { ctl->next = first; }
+
 template <typename T>
 using WaveKernel = void (*)(MixArgs<T>, const T *, T *, T *, WaveCtl *, int, int, int *);
 
@@ -1479,6 +1491,7 @@ static jci_status launch_wave(jci_space *s, const MixArgs<T> &m, const T *v, T *
     WaveKernel<T> kern = wave_kernel<T, 2>(TM), kern1 = wave_kernel<T, 1>(TM);
     if (!kern || !kern1) return JCI_ERR_SPACE;
     size_t smem = mix_smem(m.sa, TM, sizeof(T)), smem1 = mix_smem(m.sa, TM, sizeof(T), 1);
+    if (smem + 64 > f->smem_max) return JCI_ERR_SPACE;  // 16 bytes of static shared memory
     JCI_CUDA(smem_optin(kern));
     JCI_CUDA(smem_optin(kern1));
     int occ = 0, occ1 = 0, nsm = 0;
@@ -1501,6 +1514,10 @@ static jci_status launch_wave(jci_space *s, const MixArgs<T> &m, const T *v, T *
         JCI_CUDA(cudaMalloc(&f->wctl[prec], sizeof(WaveCtl)));
     }
     JCI_CUDA(cudaMemsetAsync(f->wctl[prec], 0, sizeof(WaveCtl), st));
+    if (f->wave_expire) {
+        f->wave_expire = 0;
+        k_wave_arm<<<1, 1, 0, st>>>((WaveCtl *)f->wctl[prec], std::min(kWaveLag, m.na) * ngi);
+    }
     kern<<<grid, kMixThreads, smem, st>>>(m, v, o, (T *)f->wbuf[prec], (WaveCtl *)f->wctl[prec],
                                           ngi, nhi, f->tc_status);
     return JCI_OK;

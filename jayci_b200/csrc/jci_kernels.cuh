@@ -12,6 +12,9 @@ bool fci_supported(const jci_space *s);
 // JCI_ERR_TIMEOUT (and the flag cleared) if a product kernel's bounded
 // device wait expired since the last call; synchronises with the device.
 jci_status fci_wait_status(jci_space *s);
+// Test hook: the next launch of the shared-panel product leaves the GEMM
+// items of its first rows undone, so that its gathers' waits expire.
+jci_status fci_arm_wait_expiry(jci_space *s);
 jci_status fci_prepare(jci_space *s);
 jci_status fci_sigma(jci_space *s, int nvec, const void *v, void *sig, long long ld,
                      int precision, cudaStream_t st);

@@ -80,3 +80,31 @@ def test_shared_panel_bench_sizes(name, prec):
     s.set_sigma_plan(prec, 6, 512, 1, 2)
     assert torch.equal(_sigma(s, v, prec), y)
     s.close()
+
+
+def test_bounded_wait_expires_and_space_recovers():
+    """A dependency that nothing satisfies (jci_test_expire_next_wait: the
+    panel work of the first two alpha rows is skipped): the gathers that
+    need it give up after their one-second bound, the kernel returns, the
+    host reads JCI_ERR_TIMEOUT, and the next sigma on the same space is
+    right again."""
+    import ctypes
+    import time
+    g = np.load(os.path.join(GOLDEN, "cas10_10.npz"))
+    s = jb.Space(*(int(x) for x in g["general"]))
+    s.set_integrals(g["m1"], g["m2"], float(g["e_nuc"]), 0.0)
+    s.set_sigma_plan(jb.FP64, 6, 256, 32, 1)
+    v = np.ascontiguousarray(g["sigma_v"][0])
+    ref = g["sigma"][0]
+    bar = BAR[jb.FP64] * np.abs(ref).max()
+    assert np.abs(s.sigma(v[None, :])[0] - ref).max() <= bar
+    L = jb.lib()
+    L.jci_test_expire_next_wait.argtypes = [ctypes.c_void_p]
+    assert L.jci_test_expire_next_wait(s.h) == 0
+    with pytest.raises(jb.JciError) as e:
+        t0 = time.time()
+        s.sigma(v[None, :])
+    assert e.value.status == 10  # JCI_ERR_TIMEOUT
+    assert 0.5 < time.time() - t0 < 60
+    assert np.abs(s.sigma(v[None, :])[0] - ref).max() <= bar
+    s.close()
