@@ -304,9 +304,10 @@ __global__ void __launch_bounds__(ITEMS <= 2 ? 1024 : 512)
 //                  + sum_{beta singles Ib -> Jb, pair q, phase t} t T[q][Jb].
 // The first two terms are the alpha single elements (hmatels_1x with the
 // beta string's Coulomb sum sum_{m in Ib} (mm|p_j)); the last is
-// hmatels_2xab summed over both strings' singles.  The product runs on the
-// FP32/FP64 CUDA-core pipes with a 16x16 thread grid, each thread holding a
-// TM x 4 register tile; T goes to a per-CTA scratch panel in global memory
+// hmatels_2xab summed over both strings' singles.  The product runs in FP64
+// on the FP64 tensor cores (mma.sync m8n8k4, 8 x 8 tiles, k in steps of 4)
+// and in FP32 on the FMA pipes (a 16x16 thread grid, each thread holding a
+// TM x 4 register tile); T goes to a per-CTA scratch panel in global memory
 // (L2-resident for the mid sizes) and is gathered back in a fixed order, so
 // results stay bitwise reproducible.
 
@@ -324,6 +325,140 @@ struct MixArgs {
     const int *skip;
 };
 
+// Shared-memory layout of the panel product: A [K4][AS] (alpha singles x
+// panel rows), B [NB][K4][BS] (alpha singles x 64 columns), jl [K].  FP64
+// runs the product on the FP64 tensor cores (mma.sync m8n8k4): K is padded
+// to a multiple of 4 with zero rows, and A and B rows are padded by 4
+// doubles so that a warp's fragment loads (rows k..k+3, 8 consecutive
+// elements each) fall in distinct banks.  FP32 keeps the unpadded layout of
+// its FMA form.
+__host__ __device__ constexpr int mix_k4(int K, int w) { return w == 8 ? (K + 3) & ~3 : K; }
+__host__ __device__ constexpr int mix_as(int TM, int w) { return 16 * TM + (w == 8 ? 4 : 0); }
+__host__ __device__ constexpr int mix_bs(int w) { return kMixCols + (w == 8 ? 4 : 0); }
+
+__device__ __forceinline__ void mix_dmma(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+// A and jl of alpha string Ia: A[j][m] = s_j (p_j | m) for the pairs m,
+// s_j a1(Ia, j) in row U = npair, zero in the padding.
+template <typename T, int TM>
+__device__ __forceinline__ void mix_build_a(const MixArgs<T> &a, int Ia, T *As, int *jl) {
+    constexpr int MP = 16 * TM, AS = mix_as(TM, sizeof(T));
+    const int K = a.sa, K4 = mix_k4(K, sizeof(T));
+    for (int idx = threadIdx.x; idx < K4 * MP; idx += kMixThreads) {
+        const int j = idx / MP, m = idx - j * MP;
+        T v = T(0);
+        if (j < K) {
+            const long long o = (long long)j * a.na + Ia;
+            const uint32_t e = a.fsA[o];
+            if (m < a.npair) v = a.m2[eri_index(a.fpA[o], m)];
+            else if (m == a.npair) v = a.a1A[o];
+            v = flip(v, e >> 31);
+            if (m == 0) jl[j] = (int)(e & 0x3fffffffu);
+        }
+        As[j * AS + m] = v;
+    }
+}
+
+// B chunk c: the 64 columns c*64.. of the rows jl of C (cp.async), zero past
+// the last column and in the padding rows; one commit group.
+template <typename T>
+__device__ __forceinline__ void mix_stage(const MixArgs<T> &a, const T *__restrict__ V,
+                                          const int *jl, int c, T *buf) {
+    constexpr int BS = mix_bs(sizeof(T));
+    const int K = a.sa, K4 = mix_k4(K, sizeof(T));
+    const int c0 = c * kMixCols;
+    for (int idx = threadIdx.x; idx < K4 * kMixCols; idx += kMixThreads) {
+        const int j = idx >> 6, cc = idx & 63, col = c0 + cc;
+        T *dst = buf + j * BS + cc;
+        if (j < K && col < a.nb)
+            __pipeline_memcpy_async(dst, V + (long long)jl[j] * a.nb + col, sizeof(T));
+        else
+            *dst = T(0);
+    }
+    __pipeline_commit();
+}
+
+// T[m][c0 + col] = sum_j A[j][m] B[j][col] for the panel rows m < mrows of
+// one 64-column chunk, into the panel row stride nbp.  FP64: warp w owns
+// columns 16 (w & 3) .. + 15 and panel rows 8 TM (w >> 2) .. + 8 TM - 1 as
+// 2 x TM tiles of 8 x 8, accumulated over k in steps of 4 by mma.sync.
+// FP32: the 16 x 16 thread grid, each thread a TM x 4 register tile.
+template <typename T, int TM>
+__device__ __forceinline__ void mix_product(const MixArgs<T> &a, const T *As, const T *Bc,
+                                            T *Tb, int c0) {
+    if constexpr (sizeof(T) == 8) {
+        constexpr int AS = mix_as(TM, 8), BS = mix_bs(8);
+        const int K4 = mix_k4(a.sa, 8);
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+        const int wn = warp & 3, wm = warp >> 2;
+        double acc[TM][2][2];
+#pragma unroll
+        for (int i = 0; i < TM; i++)
+#pragma unroll
+            for (int n = 0; n < 2; n++) acc[i][n][0] = acc[i][n][1] = 0.0;
+        const double *ap = As + t * AS + 8 * TM * wm + g;
+        const double *bp = Bc + t * BS + 16 * wn + g;
+#pragma unroll 2
+        for (int k0 = 0; k0 < K4; k0 += 4) {
+            const double b0 = bp[k0 * BS], b1 = bp[k0 * BS + 8];
+#pragma unroll
+            for (int i = 0; i < TM; i++) {
+                const double av = ap[k0 * AS + 8 * i];
+                mix_dmma(acc[i][0], av, b0);
+                mix_dmma(acc[i][1], av, b1);
+            }
+        }
+        // accumulator layout: lane holds row g, columns 2t and 2t+1 of a tile
+#pragma unroll
+        for (int i = 0; i < TM; i++) {
+            const int m = 8 * (TM * wm + i) + g;
+            if (m < a.mrows) {
+#pragma unroll
+                for (int n = 0; n < 2; n++)
+                    *reinterpret_cast<double2 *>(Tb + (size_t)m * a.nbp + c0 + 16 * wn + 8 * n +
+                                                 2 * t) = make_double2(acc[i][n][0], acc[i][n][1]);
+            }
+        }
+    } else {
+        constexpr int MP = 16 * TM;
+        const int K = a.sa, tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+        T acc[TM][4];
+#pragma unroll
+        for (int i = 0; i < TM; i++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[i][q] = T(0);
+#pragma unroll 4
+        for (int k = 0; k < K; k++) {
+            // thread tx owns columns tx, tx+16, tx+32, tx+48: a warp reads
+            // 16 consecutive words per load (no bank conflicts)
+            const T *br = Bc + k * kMixCols + tx;
+            T b0 = br[0], b1 = br[16], b2 = br[32], b3 = br[48];
+            const T *ar = As + k * MP + ty * TM;
+#pragma unroll
+            for (int i = 0; i < TM; i++) {
+                T av = ar[i];
+                acc[i][0] = fma(av, b0, acc[i][0]);
+                acc[i][1] = fma(av, b1, acc[i][1]);
+                acc[i][2] = fma(av, b2, acc[i][2]);
+                acc[i][3] = fma(av, b3, acc[i][3]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < TM; i++) {
+            int m = ty * TM + i;
+            if (m < a.mrows) {
+                T *dst = Tb + (size_t)m * a.nbp + c0 + tx;
+#pragma unroll
+                for (int q = 0; q < 4; q++) dst[16 * q] = acc[i][q];
+            }
+        }
+    }
+}
+
 // NB = 2: B chunks double-buffered (chunk c+1 copied while chunk c
 // multiplies); NB = 1: one buffer, so that two CTAs fit an SM where the
 // double-buffered form fits one (the other CTA's product then covers this
@@ -333,83 +468,31 @@ __global__ void __launch_bounds__(kMixThreads)
     k_sigma_mixed(MixArgs<T> a, const T *__restrict__ V, T *__restrict__ S, T *__restrict__ Tbuf) {
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int MP = 16 * TM;
-    const int K = a.sa;
-    T *As = reinterpret_cast<T *>(smem_raw);          // [K][MP]
-    T *Bs = As + (size_t)K * MP;                      // [NB][K][64]
-    int *jl = reinterpret_cast<int *>(Bs + NB * (size_t)K * kMixCols);  // [K]
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int K4 = mix_k4(a.sa, sizeof(T));
+    T *As = reinterpret_cast<T *>(smem_raw);                          // [K4][AS]
+    T *Bs = As + (size_t)K4 * mix_as(TM, sizeof(T));                  // [NB][K4][BS]
+    int *jl = reinterpret_cast<int *>(Bs + NB * (size_t)K4 * mix_bs(sizeof(T)));  // [K]
+    const size_t bsz = (size_t)K4 * mix_bs(sizeof(T));
+    const int tid = threadIdx.x;
     T *Tb = Tbuf + (size_t)blockIdx.x * a.mrows * a.nbp;
     const int nchunk = a.nbp / kMixCols;
-    // B chunks are double-buffered: chunk c+1 is copied (cp.async) while
-    // chunk c is multiplied
-    auto stage = [&](int c, T *buf) {
-        const int c0 = c * kMixCols;
-        for (int idx = tid; idx < K * kMixCols; idx += kMixThreads) {
-            int j = idx >> 6, col = c0 + (idx & 63);
-            if (col < a.nb)
-                __pipeline_memcpy_async(buf + idx, V + (long long)jl[j] * a.nb + col, sizeof(T));
-            else
-                buf[idx] = T(0);
-        }
-        __pipeline_commit();
-    };
     for (int Ia = blockIdx.x; Ia < a.na; Ia += gridDim.x) {
         __syncthreads();
-        for (int idx = tid; idx < K * MP; idx += kMixThreads) {
-            int j = idx / MP, m = idx - j * MP;
-            long long o = (long long)j * a.na + Ia;
-            uint32_t e = a.fsA[o];
-            T v = T(0);
-            if (m < a.npair) v = a.m2[eri_index(a.fpA[o], m)];
-            else if (m == a.npair) v = a.a1A[o];
-            As[idx] = flip(v, e >> 31);
-            if (m == 0) jl[j] = (int)(e & 0x3fffffffu);
-        }
+        mix_build_a<T, TM>(a, Ia, As, jl);
         __syncthreads();
-        stage(0, Bs);
+        mix_stage<T>(a, V, jl, 0, Bs);
         for (int ci = 0; ci < nchunk; ci++) {
-            const int c0 = ci * kMixCols;
-            T *Bc = Bs + (size_t)(NB == 2 ? (ci & 1) : 0) * K * kMixCols;
+            T *Bc = Bs + (NB == 2 ? (ci & 1) : 0) * bsz;
             if (NB == 2 && ci + 1 < nchunk) {
-                stage(ci + 1, Bs + (size_t)((ci + 1) & 1) * K * kMixCols);
+                mix_stage<T>(a, V, jl, ci + 1, Bs + ((ci + 1) & 1) * bsz);
                 __pipeline_wait_prior(1);
             } else {
                 __pipeline_wait_prior(0);
             }
             __syncthreads();
-            T acc[TM][4];
-#pragma unroll
-            for (int i = 0; i < TM; i++)
-#pragma unroll
-                for (int q = 0; q < 4; q++) acc[i][q] = T(0);
-#pragma unroll 4
-            for (int k = 0; k < K; k++) {
-                // thread tx owns columns tx, tx+16, tx+32, tx+48: a warp
-                // reads 16 consecutive words per load (no bank conflicts)
-                const T *br = Bc + k * kMixCols + tx;
-                T b0 = br[0], b1 = br[16], b2 = br[32], b3 = br[48];
-                const T *ar = As + k * MP + ty * TM;
-#pragma unroll
-                for (int i = 0; i < TM; i++) {
-                    T av = ar[i];
-                    acc[i][0] = fma(av, b0, acc[i][0]);
-                    acc[i][1] = fma(av, b1, acc[i][1]);
-                    acc[i][2] = fma(av, b2, acc[i][2]);
-                    acc[i][3] = fma(av, b3, acc[i][3]);
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < TM; i++) {
-                int m = ty * TM + i;
-                if (m < a.mrows) {
-                    T *dst = Tb + (size_t)m * a.nbp + c0 + tx;
-#pragma unroll
-                    for (int q = 0; q < 4; q++) dst[16 * q] = acc[i][q];
-                }
-            }
+            mix_product<T, TM>(a, As, Bc, Tb, ci * kMixCols);
             __syncthreads();
-            if (NB == 1 && ci + 1 < nchunk) stage(ci + 1, Bs);
+            if (NB == 1 && ci + 1 < nchunk) mix_stage<T>(a, V, jl, ci + 1, Bs);
         }
         // gather: every column of the row owned by one thread, fixed order.
         // The panel reads are random (DRAM once the panels outgrow L2); the
@@ -629,28 +712,17 @@ __global__ void __launch_bounds__(kMixThreads)
     if (a.skip && *a.skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_item, s_ok;
-    constexpr int MP = 16 * TM;
-    const int K = a.sa;
-    T *As = reinterpret_cast<T *>(smem_raw);          // [K][MP]
-    T *Bs = As + (size_t)K * MP;                      // [NB][K][64]
-    int *jl = reinterpret_cast<int *>(Bs + NB * (size_t)K * kMixCols);  // [K]
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int K4 = mix_k4(a.sa, sizeof(T));
+    T *As = reinterpret_cast<T *>(smem_raw);                          // [K4][AS]
+    T *Bs = As + (size_t)K4 * mix_as(TM, sizeof(T));                  // [NB][K4][BS]
+    int *jl = reinterpret_cast<int *>(Bs + NB * (size_t)K4 * mix_bs(sizeof(T)));  // [K]
+    const size_t bsz = (size_t)K4 * mix_bs(sizeof(T));
+    const int tid = threadIdx.x;
     const int nchunk = a.nbp / kMixCols;
     const size_t panel = (size_t)a.mrows * a.nbp;
     const int lag = min(kWaveLag, a.na), per = ngi + nhi;
     const long long pre = (long long)lag * ngi, mid = (long long)(a.na - lag) * per;
     const long long total = (long long)a.na * per;
-    auto stage = [&](int c, T *buf) {
-        const int c0 = c * kMixCols;
-        for (int idx = tid; idx < K * kMixCols; idx += kMixThreads) {
-            int j = idx >> 6, col = c0 + (idx & 63);
-            if (col < a.nb)
-                __pipeline_memcpy_async(buf + idx, V + (long long)jl[j] * a.nb + col, sizeof(T));
-            else
-                buf[idx] = T(0);
-        }
-        __pipeline_commit();
-    };
     for (;;) {
         __syncthreads();  // the previous item is done with shared memory
         if (tid == 0) s_item = atomicAdd(&ctl->next, 1);
@@ -685,60 +757,22 @@ __global__ void __launch_bounds__(kMixThreads)
         __syncthreads();
         if (!s_ok) return;
         if (gemm) {
-            const int Ia = row;
-            for (int idx = tid; idx < K * MP; idx += kMixThreads) {
-                int j = idx / MP, m = idx - j * MP;
-                long long o = (long long)j * a.na + Ia;
-                uint32_t e = a.fsA[o];
-                T v = T(0);
-                if (m < a.npair) v = a.m2[eri_index(a.fpA[o], m)];
-                else if (m == a.npair) v = a.a1A[o];
-                As[idx] = flip(v, e >> 31);
-                if (m == 0) jl[j] = (int)(e & 0x3fffffffu);
-            }
+            mix_build_a<T, TM>(a, row, As, jl);
             __syncthreads();
             const int c_lo = sub * kWaveChunks, c_hi = min(nchunk, c_lo + kWaveChunks);
-            stage(c_lo, Bs);
+            mix_stage<T>(a, V, jl, c_lo, Bs);
             for (int ci = c_lo; ci < c_hi; ci++) {
-                const int c0 = ci * kMixCols;
-                T *Bc = Bs + (size_t)(NB == 2 ? ((ci - c_lo) & 1) : 0) * K * kMixCols;
+                T *Bc = Bs + (NB == 2 ? ((ci - c_lo) & 1) : 0) * bsz;
                 if (NB == 2 && ci + 1 < c_hi) {
-                    stage(ci + 1, Bs + (size_t)((ci + 1 - c_lo) & 1) * K * kMixCols);
+                    mix_stage<T>(a, V, jl, ci + 1, Bs + ((ci + 1 - c_lo) & 1) * bsz);
                     __pipeline_wait_prior(1);
                 } else {
                     __pipeline_wait_prior(0);
                 }
                 __syncthreads();
-                T acc[TM][4];
-#pragma unroll
-                for (int i = 0; i < TM; i++)
-#pragma unroll
-                    for (int qq = 0; qq < 4; qq++) acc[i][qq] = T(0);
-#pragma unroll 4
-                for (int k = 0; k < K; k++) {
-                    const T *br = Bc + k * kMixCols + tx;
-                    T b0 = br[0], b1 = br[16], b2 = br[32], b3 = br[48];
-                    const T *ar = As + k * MP + ty * TM;
-#pragma unroll
-                    for (int i = 0; i < TM; i++) {
-                        T av = ar[i];
-                        acc[i][0] = fma(av, b0, acc[i][0]);
-                        acc[i][1] = fma(av, b1, acc[i][1]);
-                        acc[i][2] = fma(av, b2, acc[i][2]);
-                        acc[i][3] = fma(av, b3, acc[i][3]);
-                    }
-                }
-#pragma unroll
-                for (int i = 0; i < TM; i++) {
-                    int m = ty * TM + i;
-                    if (m < a.mrows) {
-                        T *dst = Tb + (size_t)m * a.nbp + c0 + tx;
-#pragma unroll
-                        for (int qq = 0; qq < 4; qq++) dst[16 * qq] = acc[i][qq];
-                    }
-                }
+                mix_product<T, TM>(a, As, Bc, Tb, ci * kMixCols);
                 __syncthreads();
-                if (NB == 1 && ci + 1 < c_hi) stage(ci + 1, Bs);
+                if (NB == 1 && ci + 1 < c_hi) mix_stage<T>(a, V, jl, ci + 1, Bs);
             }
             // release (the pattern of a grid barrier): the CTA's panel stores,
             // then one thread's fence and count
@@ -1213,8 +1247,12 @@ static size_t rows_smem(int nb, int npair, int da, int RB, size_t w) {
     return (size_t)RB * nb * w + (size_t)RB * npair * w + (size_t)RB * da * (w + 4) + 16;
 }
 
+// Dynamic shared memory of k_sigma_mixed / k_sigma_wave (nb B buffers); it
+// also covers k_sigma_mixed_blk's unpadded layout with two buffers.
 static size_t mix_smem(int K, int TM, size_t w, int nb = 2) {
-    return (size_t)K * 16 * TM * w + (size_t)nb * K * kMixCols * w + (size_t)K * 4 + 16;
+    const int K4 = mix_k4(K, (int)w);
+    return (size_t)K4 * mix_as(TM, (int)w) * w + (size_t)nb * K4 * mix_bs((int)w) * w +
+           (size_t)K * 4 + 16;
 }
 
 static size_t fci_smem(int nb, int npair, int R, size_t w) {
