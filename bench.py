@@ -90,7 +90,9 @@ def sigma_plan_desc(mode, nt, R, B, ms=None):
                               "256-column blocks" if R >= 16 else "whole alpha row per CTA")
     if groups:
         d["group_kernel"] = (f"{B} column(s) per thread" if B <= 2 else
-                             f"targets split over 4 warps, {5 - B} column(s) per lane")
+                             f"targets split over 4 warps, {5 - B} column(s) per lane" if B <= 4
+                             else "hole-string pair products, " +
+                             ("widest column blocks" if B == 5 else "64-column blocks"))
     else:
         d["beta_pass_threads" if streams else "rows_per_cta"] = B
     if ms is not None:

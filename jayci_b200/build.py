@@ -26,7 +26,7 @@ EXE = os.path.join(HERE, "jci")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["jci_space.cpp", "jci_io.cpp", "jci_api.cpp", "jci_server.cpp", "jci_device.cu", "jci_fci.cu",
-           "jci_fci_ab.cu", "jci_fci_tc.cu", "jci_fci_group.cu", "jci_davidson.cu", "jci_dyson.cu"]
+           "jci_fci_ab.cu", "jci_fci_tc.cu", "jci_fci_group.cu", "jci_fci_pairs.cu", "jci_davidson.cu", "jci_dyson.cu"]
 # driver programs: (source, executable)
 PROGRAMS = [("jci_main.c", "jci"), ("jci_dyson_main.c", "jci_dyson")]
 

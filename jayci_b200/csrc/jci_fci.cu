@@ -65,6 +65,10 @@ struct FciTables {
     void *wbuf[2] = {nullptr, nullptr};   // row-shared panels of the queued product
     void *wctl[2] = {nullptr, nullptr};   // and its queue counters (WaveCtl)
     int wave_expire = 0;           // test hook: the next such launch skips work (see below)
+    PairTables prs[2];             // same-spin doubles through hole strings, per spin
+    int prs_state = 0;             // 0 not built, 1 built, -1 not possible for this space
+    void *pbuf[2] = {nullptr, nullptr};  // their E blocks, per precision
+    size_t pbytes[2] = {0, 0};
 };
 
 bool fci_supported(const jci_space *s) {
@@ -112,6 +116,10 @@ void fci_free(DeviceState *d) {
     ab_tables_free(&f->ab[1]);
     group_tables_free(&f->grp[0]);
     group_tables_free(&f->grp[1]);
+    pair_tables_free(&f->prs[0]);
+    pair_tables_free(&f->prs[1]);
+    cudaFree(f->pbuf[0]);
+    cudaFree(f->pbuf[1]);
     delete f;
     d->fci = nullptr;
 }
@@ -1327,9 +1335,14 @@ jci_status fci_prepare(jci_space *s) {
             X.nstr, X.nelec, X.max_sing, X.max_doub, d->npair, t.istr, t.doub, t.a1, d->m2,
             f->d[sp].a1T, f->f[sp].a1T, f->d[sp].joccT, f->f[sp].joccT, f->dblJ[sp],
             f->d[sp].dblH, f->f[sp].dblH);
-        // the group coefficient blocks follow the current double values
+        // the group coefficient blocks and the pair matrices follow the
+        // current integrals
         if (f->grp[sp].uidx) {
             jci_status r = group_fill(&f->grp[sp], f->d[sp].dblH, f->f[sp].dblH, st);
+            if (r) return r;
+        }
+        if (f->prs[sp].jrow) {
+            jci_status r = pair_fill(s, &f->prs[sp], st);
             if (r) return r;
         }
     }
@@ -1745,13 +1758,75 @@ static jci_status group_tables(jci_space *s, cudaStream_t st) {
 
 static bool group_possible(const FciTables *f) { return f->da >= 1 && f->db >= 1; }
 
-// Doubles of spin sp by groups: rows x len matrix x -> y (add: y += ...),
-// with the diagonal hd when given; items = the group kernel variant (1-4,
-// group_launch).
+// Hole-string tables of both spins (jci_fci_pairs.cu), built and filled on
+// first use (not while a stream is being captured); JCI_ERR_SPACE, and
+// remembered, for spaces they do not cover.
+static jci_status pair_tables(jci_space *s, cudaStream_t st) {
+    FciTables *f = s->dev->fci;
+    if (f->prs_state > 0) return JCI_OK;
+    if (f->prs_state < 0) return JCI_ERR_SPACE;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    JCI_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return JCI_ERR_STATE;
+    jci_status r = JCI_OK;
+    for (int sp = 0; sp < 2 && !r; sp++) {
+        r = pair_tables_build(s, sp, &f->prs[sp]);
+        if (!r) r = pair_fill(s, &f->prs[sp], st);
+        if (!r && pair_smem_bytes(f->prs[sp], 0) > f->smem_max) r = JCI_ERR_SPACE;
+    }
+    if (r) {
+        pair_tables_free(&f->prs[0]);
+        pair_tables_free(&f->prs[1]);
+        f->prs_state = r == JCI_ERR_SPACE ? -1 : 0;
+        return r;
+    }
+    f->prs_state = 1;
+    return JCI_OK;
+}
+
+// E block of the hole-string doubles for variant `items` (5, 6) in this
+// precision, grown on demand (not while a stream is being captured).
+template <typename T>
+static jci_status pair_scratch(jci_space *s, int items, cudaStream_t st, T **E) {
+    FciTables *f = s->dev->fci;
+    const int prec = sizeof(T) == 8 ? 0 : 1;
+    size_t need = 0;
+    for (int sp = 0; sp < 2; sp++) {
+        const PairTables &t = f->prs[sp];
+        const int len = sp == 0 ? f->nb : f->na;
+        need = std::max(need, (size_t)t.nk * t.np * pair_block_cols(t, len, items, sizeof(T)) *
+                                  sizeof(T));
+    }
+    if (f->pbytes[prec] < need) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        JCI_CUDA(cudaStreamIsCapturing(st, &cs));
+        if (cs != cudaStreamCaptureStatusNone) return JCI_ERR_STATE;
+        JCI_CUDA(cudaFree(f->pbuf[prec]));
+        f->pbuf[prec] = nullptr;
+        f->pbytes[prec] = 0;
+        JCI_CUDA(cudaMalloc(&f->pbuf[prec], need));
+        f->pbytes[prec] = need;
+    }
+    *E = (T *)f->pbuf[prec];
+    return JCI_OK;
+}
+
+// Doubles of spin sp: rows x len matrix x -> y (add: y += ...), with the
+// diagonal hd when given; items = the variant: 1-4 the string-group kernel
+// (group_launch), 5, 6 the hole-string products (pair_launch: widest
+// column block, 64-column blocks).
 template <typename T>
 static jci_status launch_group(jci_space *s, int sp, const T *hd, int add, const int *skip,
                                int items, const T *x, T *y, cudaStream_t st) {
     FciTables *f = s->dev->fci;
+    if (items >= 5) {
+        jci_status r = pair_tables(s, st);
+        T *E = nullptr;
+        if (!r) r = pair_scratch<T>(s, items, st, &E);
+        if (r) return r;
+        return pair_launch<T>(f->prs[sp], sp == 0 ? f->nb : f->na, items, x, y, hd, add, skip, E,
+                              s->dev->device, st);
+    }
     jci_status r = group_tables(s, st);
     if (r) return r;
     const GroupTables &t = f->grp[sp];
@@ -2018,7 +2093,9 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
             if (ms < bs) { bs = ms; b6s = nt; }
         }
         float gg = 1e30f;
-        for (int it : {1, 2, 3, 4}) {
+        const bool pairs = pair_tables(s, st) == JCI_OK;
+        for (int it : {1, 2, 3, 4, 5, 6}) {
+            if (it >= 5 && !pairs) continue;
             float ms = timeit([&] {
                 jci_status q = launch_group<T>(s, 1, nullptr, 1, nullptr, it, ct, tau, st);
                 return q ? q : launch_group<T>(s, 0, a.hd, 0, nullptr, it, v, o, st);
@@ -2161,9 +2238,10 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, 
     size_t w = p ? sizeof(float) : sizeof(double);
     if (mode == 6 || mode == 7) {
         bool ok = mode == 6 ? mixed_possible(f, w) && R >= 0 : ab_plan_possible(f, R, w);
-        if (!ok || !group_possible(f) || !stream_ok(f->na, nt) || B < 1 || B > 4 ||
+        if (!ok || !group_possible(f) || !stream_ok(f->na, nt) || B < 1 || B > 6 ||
             stream_smem(0, f->sb, w) > f->smem_max)
             return JCI_ERR_ARG;
+        if (B >= 5 && pair_tables(s, s->dev->stream) != JCI_OK) return JCI_ERR_ARG;
     } else if (mode == 3 || mode == 4) {
         bool ok = mode == 3 ? mixed_possible(f, w) && R >= 0 : ab_plan_possible(f, R, w);
         if (!ok || !stream_ok(f->nb, nt) || !stream_ok(f->na, B) ||
@@ -2188,7 +2266,7 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, 
         if (r) return r;
     }
     if (mode == 6 || mode == 7) {
-        jci_status r = group_tables(s, s->dev->stream);
+        jci_status r = B >= 5 ? JCI_OK : group_tables(s, s->dev->stream);
         if (r) return r;
     }
     if ((mode == 1 || mode == 3 || mode == 6) && R >= 16 && R < 32) {  // column-blocked lists

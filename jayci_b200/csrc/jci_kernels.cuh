@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "jci_device.cuh"
 
 namespace jci {
@@ -93,6 +95,28 @@ jci_status group_fill(GroupTables *t, const double *dblH, const float *dblHf, cu
 template <typename T>
 jci_status group_launch(const GroupArgs<T> &a, int items, int device, const T *x, T *y,
                         cudaStream_t st);
+
+// Same-spin doubles through (N-2)-electron hole strings, jci_fci_pairs.cu
+// (group kernel variants 5 and 6).
+struct PairTables {
+    int nk = 0, np = 0, NP = 0, nt = 0, ngp = 0, rows = 0;
+    std::vector<int> orb;          // the varying orbitals (1-based)
+    int *jrow = nullptr;           // [hole string][pair] source string | phase << 31
+    uint16_t *gp = nullptr;        // [hole string][pair] orbital pair
+    int *pull = nullptr;           // [string][hole] hole string * np + pair
+    double *W64 = nullptr;         // [orbital pair][orbital pair]
+    float *W32 = nullptr;
+    std::vector<double> w64;       // host copies behind the asynchronous uploads
+    std::vector<float> w32;
+};
+jci_status pair_tables_build(const jci_space *s, int spin, PairTables *t);
+jci_status pair_fill(const jci_space *s, PairTables *t, cudaStream_t st);
+void pair_tables_free(PairTables *t);
+size_t pair_smem_bytes(const PairTables &t, int prec);
+int pair_block_cols(const PairTables &t, int len, int variant, size_t w);
+template <typename T>
+jci_status pair_launch(const PairTables &t, int len, int variant, const T *x, T *y, const T *hd,
+                       int add, const int *skip, T *E, int device, cudaStream_t st);
 
 // Generic path (any truncated space), jci_device.cu.
 jci_status device_sigma_generic(jci_space *s, int nvec, const void *vin, void *sout,

@@ -53,6 +53,8 @@ def test_plan_description_names_each_plans_parameters():
     assert bench.sigma_plan_desc(6, 512, 2, 2)["product_panel"] == "whole alpha row per CTA"
     assert "1 column" in bench.sigma_plan_desc(6, 256, 0, 1)["group_kernel"]
     assert "split over 4 warps, 1 column" in bench.sigma_plan_desc(6, 256, 0, 4)["group_kernel"]
+    assert "hole-string" in bench.sigma_plan_desc(6, 256, 0, 5)["group_kernel"]
+    assert "64-column" in bench.sigma_plan_desc(7, 256, 16, 6)["group_kernel"]
     d = bench.sigma_plan_desc(3, 256, 0, 512)
     assert d["alpha_pass_threads"] == 256 and d["beta_pass_threads"] == 512
     d = bench.sigma_plan_desc(5, 256, 16, 2)

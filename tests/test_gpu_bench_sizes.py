@@ -132,7 +132,9 @@ def test_every_plan_at_fci12(prec):
              (7, 512, 16, 1), (7, 512, 16, 2), (7, 512, 16, 3), (7, 512, 16, 4),
              (7, 512, 8, 3),
              # the column-blocked panel (product CTAs per SM + 16)
-             (1, 256, 17, 2), (3, 256, 16, 256), (6, 512, 18, 2)]
+             (1, 256, 17, 2), (3, 256, 16, 256), (6, 512, 18, 2),
+             # the same-spin doubles through hole strings (variants 5, 6)
+             (6, 512, 0, 5), (6, 512, 2, 6), (7, 512, 16, 5)]
     ran = 0
     for plan in plans:
         try:
