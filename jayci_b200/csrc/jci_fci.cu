@@ -2080,6 +2080,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     // modes 6, 7: the doubles by string groups, the beta singles as a stream
     float best6 = 1e30f;
     int b6s = 0, b6i = 1;
+    bool pairs = false;  // the hole-string variants (5, 6) can run
     if (bsprod < 1e30f && group_possible(f) && !err) {
         T *ct = nullptr, *tau = nullptr;
         err = stream_scratch<T>(f, &ct, &tau);
@@ -2093,7 +2094,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
             if (ms < bs) { bs = ms; b6s = nt; }
         }
         float gg = 1e30f;
-        const bool pairs = pair_tables(s, st) == JCI_OK;
+        pairs = pair_tables(s, st) == JCI_OK;
         for (int it : {1, 2, 3, 4, 5, 6}) {
             if (it >= 5 && !pairs) continue;
             float ms = timeit([&] {
@@ -2129,7 +2130,8 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
         // every group kernel variant, end to end (their component timings
         // are close and noisy)
         best6 = 1e30f;
-        for (int it : {1, 2, 3, 4}) {
+        for (int it : {1, 2, 3, 4, 5, 6}) {
+            if (it >= 5 && !pairs) continue;
             float ms = best_of([&] { return run_plan<T>(s, a, gmode, b6s, sR, it, v, o, st); });
             if (ms < best6) { best6 = ms; b6i = it; }
         }
