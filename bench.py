@@ -86,7 +86,9 @@ def sigma_plan_desc(mode, nt, R, B, ms=None):
                                f"{R} column threads")
     else:
         d["product_ctas_per_sm"] = R % 16
-        d["product_panel"] = ("one per alpha row, shared by all CTAs (L2)" if R >= 32 else
+        d["product_panel"] = ("whole alpha row per CTA, compact (the entries the gather reads)"
+                              if R >= 64 else
+                              "one per alpha row, shared by all CTAs (L2)" if R >= 32 else
                               "256-column blocks" if R >= 16 else "whole alpha row per CTA")
     if groups:
         d["group_kernel"] = (f"{B} column(s) per thread" if B <= 2 else
@@ -130,9 +132,11 @@ def profile_key(mode, R, B):
     the string-group plans (6, 7) also the group kernel variant ("7:3"); for
     the panel products (1, 3, 6) a ":blk" suffix when the panel is cut into
     column blocks (16 <= R < 32), ":row" when one panel per alpha row is
-    shared by all CTAs (R >= 32)."""
+    shared by all CTAs (32 <= R < 64), ":cp" for the compact panel (R >= 64)."""
     key = f"{mode}:{B}" if mode in (6, 7) else str(mode)
-    if mode in (1, 3, 6) and R >= 32:
+    if mode in (1, 3, 6) and R >= 64:
+        key += ":cp"
+    elif mode in (1, 3, 6) and R >= 32:
         key += ":row"
     elif mode in (1, 3, 6) and R >= 16:
         key += ":blk"

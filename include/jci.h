@@ -208,14 +208,18 @@ jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sigma,
  * (mode 0: alpha rows staged per pass; modes 1-3 and 6: product CTAs per
  * SM, 0 = as many as fit, plus 16 for the panel cut into 256-column blocks
  * gathered block by block, plus 32 for one panel per alpha row built and
- * gathered by all CTAs from a shared work queue (modes 1, 3, 6); modes 4,
+ * gathered by all CTAs from a shared work queue, plus 64 for the per-CTA
+ * panel stored compact (only the entries its gather reads) (modes 1, 3,
+ * 6); modes 4,
  * 5, 7: column threads of the fused
  * product, 8 (CUDA cores, 32-column chunks) or 16 (tensor cores, 64-column
  * chunks: FP64 mma.sync in FP64, 3xTF32 in FP32), or in FP32 32 / 64 (the
  * tcgen05 engine, 32- / 64-column chunks)), `batch` (modes 1, 2, 5: alpha strings per CTA of the
  * row kernel; modes 3-4: threads per CTA of the beta pass; modes 6-7: the
  * group kernel variant, 1 or 2 columns per thread, or 3, 4: the group's
- * excitation targets split over 4 warps with 2 or 1 columns per lane), and
+ * excitation targets split over 4 warps with 2 or 1 columns per lane, or
+ * 5, 6: the same-spin doubles as dense products over (N-2)-electron hole
+ * strings, in the widest or in 64-column blocks), and
  * its timed cost in
  * ms per vector.  All 0 before the first sigma call and on the
  * multi-group path.  No reference counterpart (the reference has no device

@@ -65,6 +65,12 @@ struct FciTables {
     void *wbuf[2] = {nullptr, nullptr};   // row-shared panels of the queued product
     void *wctl[2] = {nullptr, nullptr};   // and its queue counters (WaveCtl)
     int wave_expire = 0;           // test hook: the next such launch skips work (see below)
+    // compact product panel: per chunk and panel row the needed columns and
+    // the first position, the gather's entry positions per beta string
+    uint64_t *cp_mask = nullptr;
+    int *cp_base = nullptr, *cp_gidx = nullptr;
+    long long cp_len = 0;
+    int cp_ent = 0, cp_state = 0;  // cp_state 0 not built, 1 built, -1 not possible
     PairTables prs[2];             // same-spin doubles through hole strings, per spin
     int prs_state = 0;             // 0 not built, 1 built, -1 not possible for this space
     void *pbuf[2] = {nullptr, nullptr};  // their E blocks, per precision
@@ -118,6 +124,9 @@ void fci_free(DeviceState *d) {
     group_tables_free(&f->grp[1]);
     pair_tables_free(&f->prs[0]);
     pair_tables_free(&f->prs[1]);
+    cudaFree(f->cp_mask);
+    cudaFree(f->cp_base);
+    cudaFree(f->cp_gidx);
     cudaFree(f->pbuf[0]);
     cudaFree(f->pbuf[1]);
     delete f;
@@ -331,6 +340,16 @@ struct MixArgs {
     const T *m2;
     const uint64_t *occB;
     const int *skip;
+    // compact panel (null: the full mrows x nbp panel): only the entries the
+    // gather reads are stored, row after row; cmask[c][m] marks the needed
+    // columns of chunk c in panel row m, cbase[c][m] is the position of the
+    // first of them, gidx[e][Ib] the gather's entries of string Ib in its
+    // summation order (phase in bit 31), gent of them per string
+    const uint64_t *cmask = nullptr;
+    const int *cbase = nullptr;
+    const int *gidx = nullptr;
+    int gent = 0;
+    long long plen = 0;  // compact panel entries per alpha row
 };
 
 // Shared-memory layout of the panel product: A [K4][AS] (alpha singles x
@@ -395,9 +414,18 @@ __device__ __forceinline__ void mix_stage(const MixArgs<T> &a, const T *__restri
 // columns 16 (w & 3) .. + 15 and panel rows 8 TM (w >> 2) .. + 8 TM - 1 as
 // 2 x TM tiles of 8 x 8, accumulated over k in steps of 4 by mma.sync.
 // FP32: the 16 x 16 thread grid, each thread a TM x 4 register tile.
+// Position of panel entry (m, chunk column cc) in the compact panel, or -1
+// when the gather never reads it (cm, cb: the chunk's masks and bases).
+__device__ __forceinline__ int mix_cpos(const uint64_t *cm, const int *cb, int m, int cc) {
+    const uint64_t w = cm[m];
+    if (!((w >> cc) & 1)) return -1;
+    return cb[m] + __popcll(w & ((1ull << cc) - 1));
+}
+
 template <typename T, int TM>
 __device__ __forceinline__ void mix_product(const MixArgs<T> &a, const T *As, const T *Bc,
-                                            T *Tb, int c0) {
+                                            T *Tb, int c0, const uint64_t *cm = nullptr,
+                                            const int *cb = nullptr) {
     if constexpr (sizeof(T) == 8) {
         constexpr int AS = mix_as(TM, 8), BS = mix_bs(8);
         const int K4 = mix_k4(a.sa, 8);
@@ -426,9 +454,19 @@ __device__ __forceinline__ void mix_product(const MixArgs<T> &a, const T *As, co
             const int m = 8 * (TM * wm + i) + g;
             if (m < a.mrows) {
 #pragma unroll
-                for (int n = 0; n < 2; n++)
-                    *reinterpret_cast<double2 *>(Tb + (size_t)m * a.nbp + c0 + 16 * wn + 8 * n +
-                                                 2 * t) = make_double2(acc[i][n][0], acc[i][n][1]);
+                for (int n = 0; n < 2; n++) {
+                    const int cc = 16 * wn + 8 * n + 2 * t;
+                    if (cm) {
+#pragma unroll
+                        for (int e = 0; e < 2; e++) {
+                            const int q = mix_cpos(cm, cb, m, cc + e);
+                            if (q >= 0) Tb[q] = acc[i][n][e];
+                        }
+                    } else {
+                        *reinterpret_cast<double2 *>(Tb + (size_t)m * a.nbp + c0 + cc) =
+                            make_double2(acc[i][n][0], acc[i][n][1]);
+                    }
+                }
             }
         }
     } else {
@@ -459,9 +497,17 @@ __device__ __forceinline__ void mix_product(const MixArgs<T> &a, const T *As, co
         for (int i = 0; i < TM; i++) {
             int m = ty * TM + i;
             if (m < a.mrows) {
-                T *dst = Tb + (size_t)m * a.nbp + c0 + tx;
+                if (cm) {
 #pragma unroll
-                for (int q = 0; q < 4; q++) dst[16 * q] = acc[i][q];
+                    for (int q = 0; q < 4; q++) {
+                        const int p = mix_cpos(cm, cb, m, tx + 16 * q);
+                        if (p >= 0) Tb[p] = acc[i][q];
+                    }
+                } else {
+                    T *dst = Tb + (size_t)m * a.nbp + c0 + tx;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) dst[16 * q] = acc[i][q];
+                }
             }
         }
     }
@@ -480,9 +526,13 @@ __global__ void __launch_bounds__(kMixThreads)
     T *As = reinterpret_cast<T *>(smem_raw);                          // [K4][AS]
     T *Bs = As + (size_t)K4 * mix_as(TM, sizeof(T));                  // [NB][K4][BS]
     int *jl = reinterpret_cast<int *>(Bs + NB * (size_t)K4 * mix_bs(sizeof(T)));  // [K]
+    // compact panel: the chunk's masks and bases, [mrows] each
+    uint64_t *cm = reinterpret_cast<uint64_t *>(jl + ((a.sa + 1) & ~1));
+    int *cb = reinterpret_cast<int *>(cm + a.mrows);
+    const bool cp = a.cmask != nullptr;
     const size_t bsz = (size_t)K4 * mix_bs(sizeof(T));
     const int tid = threadIdx.x;
-    T *Tb = Tbuf + (size_t)blockIdx.x * a.mrows * a.nbp;
+    T *Tb = Tbuf + (size_t)blockIdx.x * (cp ? (size_t)a.plen : (size_t)a.mrows * a.nbp);
     const int nchunk = a.nbp / kMixCols;
     for (int Ia = blockIdx.x; Ia < a.na; Ia += gridDim.x) {
         __syncthreads();
@@ -497,8 +547,13 @@ __global__ void __launch_bounds__(kMixThreads)
             } else {
                 __pipeline_wait_prior(0);
             }
+            if (cp)
+                for (int m = tid; m < a.mrows; m += kMixThreads) {
+                    cm[m] = a.cmask[(size_t)ci * a.mrows + m];
+                    cb[m] = a.cbase[(size_t)ci * a.mrows + m];
+                }
             __syncthreads();
-            mix_product<T, TM>(a, As, Bc, Tb, ci * kMixCols);
+            mix_product<T, TM>(a, As, Bc, Tb, ci * kMixCols, cp ? cm : nullptr, cb);
             __syncthreads();
             if (NB == 1 && ci + 1 < nchunk) mix_stage<T>(a, V, jl, ci + 1, Bs);
         }
@@ -506,8 +561,32 @@ __global__ void __launch_bounds__(kMixThreads)
         // The panel reads are random (DRAM once the panels outgrow L2); the
         // singles loop takes its indices 8 at a time so that 8 panel reads
         // are in flight per thread, and adds them in list order.
-        const T *TU = Tb + (size_t)a.npair * a.nbp;
         T *srow = S + (long long)Ia * a.nb;
+        if (cp) {
+            // the same terms in the same order, at their compact positions
+            for (int Ib = tid; Ib < a.nb; Ib += kMixThreads) {
+                const int *gi = a.gidx + Ib;
+                T x = Tb[gi[0]];
+                int e = 1;
+                for (; e + 8 <= a.gent; e += 8) {
+                    T t[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        const int g = gi[(size_t)(e + u) * a.nb];
+                        t[u] = flip(Tb[g & 0x7fffffff], (uint32_t)g >> 31);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; u++) x += t[u];
+                }
+                for (; e < a.gent; e++) {
+                    const int g = gi[(size_t)e * a.nb];
+                    x += flip(Tb[g & 0x7fffffff], (uint32_t)g >> 31);
+                }
+                srow[Ib] += x;
+            }
+            continue;
+        }
+        const T *TU = Tb + (size_t)a.npair * a.nbp;
         for (int Ib = tid; Ib < a.nb; Ib += kMixThreads) {
             T x = TU[Ib];
             uint64_t oc = a.occB[Ib];
@@ -1255,12 +1334,13 @@ static size_t rows_smem(int nb, int npair, int da, int RB, size_t w) {
     return (size_t)RB * nb * w + (size_t)RB * npair * w + (size_t)RB * da * (w + 4) + 16;
 }
 
-// Dynamic shared memory of k_sigma_mixed / k_sigma_wave (nb B buffers); it
-// also covers k_sigma_mixed_blk's unpadded layout with two buffers.
-static size_t mix_smem(int K, int TM, size_t w, int nb = 2) {
+// Dynamic shared memory of k_sigma_mixed / k_sigma_wave (nb B buffers; with
+// the compact panel, cp_rows = mrows chunk masks and bases); it also covers
+// k_sigma_mixed_blk's unpadded layout with two buffers.
+static size_t mix_smem(int K, int TM, size_t w, int nb = 2, int cp_rows = 0) {
     const int K4 = mix_k4(K, (int)w);
     return (size_t)K4 * mix_as(TM, (int)w) * w + (size_t)nb * K4 * mix_bs((int)w) * w +
-           (size_t)K * 4 + 16;
+           (size_t)((K + 1) & ~1) * 4 + (size_t)cp_rows * 12 + 16;
 }
 
 static size_t fci_smem(int nb, int npair, int R, size_t w) {
@@ -1574,12 +1654,88 @@ static jci_status launch_wave(jci_space *s, const MixArgs<T> &m, const T *v, T *
     return JCI_OK;
 }
 
+// Tables of the compact product panel (integral independent), built on the
+// host on first use, not while a stream is being captured.  A panel entry
+// (row m, column J) is kept iff the gather reads it: the one-body row at
+// every column, the Coulomb row (mm) at the strings that hold m, and the
+// single pair row at every single's target.  At FCI(16,16) that is 73 of
+// the 137 rows per column.  Positions run row after row, columns ascending.
+static jci_status compact_tables(jci_space *s, cudaStream_t st) {
+    FciTables *f = s->dev->fci;
+    if (f->cp_state > 0) return JCI_OK;
+    if (f->cp_state < 0) return JCI_ERR_SPACE;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    JCI_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return JCI_ERR_STATE;
+    const SpinSpace &B = s->sp[1];
+    const int nb = B.nstr, ne = B.nelec, sb = f->sb, mrows = f->npair + 1;
+    const int nchunk = (nb + kMixCols - 1) / kMixCols;
+    f->cp_state = -1;
+    for (int i = 0; i < nb; i++)
+        if (B.soff[i + 1] - B.soff[i] != sb) return JCI_ERR_SPACE;
+    // the gather's reads of string Ib, in its summation order: (row, column, phase)
+    const int gent = 1 + ne + sb;
+    std::vector<int> grow((size_t)gent * nb), gcol((size_t)gent * nb), gneg((size_t)gent * nb);
+    for (int i = 0; i < nb; i++) {
+        int e = 0;
+        auto put = [&](int row, int col, int neg) {
+            grow[(size_t)e * nb + i] = row;
+            gcol[(size_t)e * nb + i] = col;
+            gneg[(size_t)e * nb + i] = neg;
+            e++;
+        };
+        put(f->npair, i, 0);
+        // Coulomb rows in ascending orbital order (the order of the occupation bits)
+        for (int k = 0; k < ne; k++) {
+            const int o = B.istr[(size_t)i * ne + k];
+            if (o > 64) return JCI_ERR_SPACE;
+            put(pair_index(o, o), i, 0);
+        }
+        for (int k = 0; k < sb; k++) {
+            const Exc &x = B.sing[B.soff[i] + k];
+            put(pair_index(x.io0, x.fo0), x.target, x.sign < 0);
+        }
+    }
+    std::vector<uint64_t> mask((size_t)nchunk * mrows, 0);
+    for (size_t q = 0; q < grow.size(); q++)
+        mask[(size_t)(gcol[q] >> 6) * mrows + grow[q]] |= 1ull << (gcol[q] & 63);
+    // positions: row after row, chunk after chunk within a row
+    std::vector<int> base((size_t)nchunk * mrows);
+    long long pos = 0;
+    for (int m = 0; m < mrows; m++)
+        for (int c = 0; c < nchunk; c++) {
+            base[(size_t)c * mrows + m] = (int)pos;
+            pos += __builtin_popcountll(mask[(size_t)c * mrows + m]);
+        }
+    if (pos >= (1ll << 31)) return JCI_ERR_SPACE;
+    std::vector<int> gidx((size_t)gent * nb);
+    for (size_t q = 0; q < grow.size(); q++) {
+        const size_t k = (size_t)(gcol[q] >> 6) * mrows + grow[q];
+        const int p = base[k] + __builtin_popcountll(mask[k] & ((1ull << (gcol[q] & 63)) - 1));
+        gidx[q] = p | (gneg[q] ? (int)0x80000000u : 0);
+    }
+    JCI_CUDA(cudaMalloc(&f->cp_mask, mask.size() * sizeof(uint64_t)));
+    JCI_CUDA(cudaMalloc(&f->cp_base, base.size() * sizeof(int)));
+    JCI_CUDA(cudaMalloc(&f->cp_gidx, gidx.size() * sizeof(int)));
+    JCI_CUDA(cudaMemcpy(f->cp_mask, mask.data(), mask.size() * sizeof(uint64_t),
+                        cudaMemcpyHostToDevice));
+    JCI_CUDA(cudaMemcpy(f->cp_base, base.data(), base.size() * sizeof(int),
+                        cudaMemcpyHostToDevice));
+    JCI_CUDA(cudaMemcpy(f->cp_gidx, gidx.data(), gidx.size() * sizeof(int),
+                        cudaMemcpyHostToDevice));
+    f->cp_len = pos;
+    f->cp_ent = gent;
+    f->cp_state = 1;
+    return JCI_OK;
+}
+
 // Second kernel of the dense-product path.  The per-CTA scratch panels are
 // allocated on first use for the largest resident grid; `per_sm` picks the
 // CTAs per SM actually launched (0 = as many as fit), which trades latency
 // hiding against keeping the panels L2-resident.  per_sm >= 16 selects the
 // column-blocked panel (k_sigma_mixed_blk) with per_sm - 16 CTAs per SM,
-// per_sm >= 32 the row-shared panels (k_sigma_wave) with per_sm - 32.
+// per_sm >= 32 the row-shared panels (k_sigma_wave) with per_sm - 32, and
+// per_sm >= 64 the compact panel (compact_tables) with per_sm - 64.
 template <typename T>
 static jci_status launch_mixed(jci_space *s, const FciArgs<T> &fa, const T *v, T *o,
                                cudaStream_t st, int per_sm) {
@@ -1592,12 +1748,27 @@ static jci_status launch_mixed(jci_space *s, const FciArgs<T> &fa, const T *v, T
     m.fsA = fa.fsA; m.fsB = fa.fsB; m.fpA = fa.fpA; m.fpB = fa.fpB;
     m.a1A = fa.a1A; m.m2 = fa.m2; m.occB = d->t[1].occ;
     m.skip = fa.skip;
+    int cp_rows = 0;
+    if (per_sm >= 64) {
+        jci_status r = compact_tables(s, st);
+        if (r) return r;
+        m.cmask = f->cp_mask;
+        m.cbase = f->cp_base;
+        m.gidx = f->cp_gidx;
+        m.gent = f->cp_ent;
+        m.plen = f->cp_len;
+        cp_rows = m.mrows;
+        per_sm -= 64;
+        if (per_sm >= 16) return JCI_ERR_ARG;  // whole-row panels only
+    }
     if (per_sm >= 32) return launch_wave<T>(s, m, v, o, st, per_sm - 32);
     if (per_sm >= 16) return launch_mixed_blk<T>(s, m, v, o, st, per_sm - 16);
     int TM = (m.mrows + 15) / 16;
     MixKernel<T> kern = mixed_kernel<T>(TM), kern1 = mixed_kernel1<T>(TM);
     if (!kern || !kern1) return JCI_ERR_SPACE;
-    size_t smem = mix_smem(m.sa, TM, sizeof(T)), smem1 = mix_smem(m.sa, TM, sizeof(T), 1);
+    size_t smem = mix_smem(m.sa, TM, sizeof(T), 2, cp_rows),
+           smem1 = mix_smem(m.sa, TM, sizeof(T), 1, cp_rows);
+    if (smem1 > f->smem_max) return JCI_ERR_SPACE;
     JCI_CUDA(smem_optin(kern));
     JCI_CUDA(smem_optin(kern1));
     {
@@ -1624,6 +1795,11 @@ static jci_status launch_mixed(jci_space *s, const FciArgs<T> &fa, const T *v, T
     int grid = f->mix_grid[prec];
     if (per_sm > 0 && per_sm < f->mix_occ[prec])
         grid = std::max(1, std::min(grid, f->nsm * per_sm));
+    if (cp_rows) {  // no more CTAs than fit with the masks' shared memory
+        int occ = 0;
+        JCI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kMixThreads, smem));
+        grid = std::max(1, std::min(grid, f->nsm * std::max(occ, 1)));
+    }
     kern<<<grid, kMixThreads, smem, st>>>(m, v, o, (T *)f->tbuf[prec]);
     return JCI_OK;
 }
@@ -2013,7 +2189,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
     int Rpanel = 1, Rmix2 = 1, txab = 0;
     if (mixed_possible(f, w))
         // whole-row panel per CTA, column-blocked, row panels shared by all CTAs
-        for (int R : {1, 2, 4, 16 + 1, 16 + 2, 16 + 4}) {
+        for (int R : {1, 2, 4, 16 + 1, 16 + 2, 16 + 4, 64 + 1, 64 + 2, 64 + 4}) {
             float ms = timeit([&] { return launch_mixed<T>(s, ar, v, o, st, R); });
             if (ms < bpanel) { bpanel = ms; Rpanel = R; }
         }
@@ -2270,6 +2446,12 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, 
     if (mode == 6 || mode == 7) {
         jci_status r = B >= 5 ? JCI_OK : group_tables(s, s->dev->stream);
         if (r) return r;
+    }
+    if ((mode == 1 || mode == 3 || mode == 6) && (R >= 128 || (R >= 64 && R - 64 >= 16)))
+        return JCI_ERR_ARG;
+    if ((mode == 1 || mode == 3 || mode == 6) && R >= 64) {  // compact panel tables
+        jci_status r = compact_tables(s, s->dev->stream);
+        if (r) return r == JCI_ERR_SPACE ? JCI_ERR_ARG : r;
     }
     if ((mode == 1 || mode == 3 || mode == 6) && R >= 16 && R < 32) {  // column-blocked lists
         AbTables *t = nullptr;

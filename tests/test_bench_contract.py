@@ -36,7 +36,8 @@ def test_every_traffic_entry_points_at_a_committed_summary():
             mode = int(key.split(":")[0])
             assert mode in bench.PLAN_NAMES
             # group plans carry their variant, blocked and shared panels a suffix
-            assert (":" in key.replace(":blk", "").replace(":row", "")) == (mode in (6, 7))
+            assert (":" in key.replace(":blk", "").replace(":row", "").replace(":cp", "")) == \
+                (mode in (6, 7))
             assert plan["dram_bytes_per_launch"] > 0 and plan["kernels"]
             assert os.path.exists(os.path.join(bench.ROOT, plan["summary"]))
 
@@ -51,6 +52,9 @@ def test_plan_description_names_each_plans_parameters():
     d = bench.sigma_plan_desc(6, 512, 33, 2)
     assert d["product_ctas_per_sm"] == 1 and "shared by all CTAs" in d["product_panel"]
     assert bench.sigma_plan_desc(6, 512, 2, 2)["product_panel"] == "whole alpha row per CTA"
+    d = bench.sigma_plan_desc(6, 512, 66, 5)
+    assert d["product_ctas_per_sm"] == 2 and "compact" in d["product_panel"]
+    assert bench.profile_key(6, 66, 5) == "6:5:cp"
     assert "1 column" in bench.sigma_plan_desc(6, 256, 0, 1)["group_kernel"]
     assert "split over 4 warps, 1 column" in bench.sigma_plan_desc(6, 256, 0, 4)["group_kernel"]
     assert "hole-string" in bench.sigma_plan_desc(6, 256, 0, 5)["group_kernel"]
