@@ -79,6 +79,10 @@ def sigma_plan_desc(mode, nt, R, B, ms=None):
     d = {"mode": mode, "name": PLAN_NAMES[mode],
          ("alpha_pass_threads" if streams else "beta_singles_threads" if groups
           else "row_kernel_threads"): nt}
+    if groups and nt == 0:
+        d["beta_singles"] = "hole-string products"
+    elif groups:
+        d["beta_singles"] = "row stream on C^T"
     if mode == 0:
         d["staged_rows"] = R
     elif mode in (4, 5, 7):
@@ -127,13 +131,17 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_key(mode, R, B):
+def profile_key(mode, R, B, nt=None):
     """Key of a sigma plan in the committed traffic summaries: the mode; for
     the string-group plans (6, 7) also the group kernel variant ("7:3"); for
     the panel products (1, 3, 6) a ":blk" suffix when the panel is cut into
     column blocks (16 <= R < 32), ":row" when one panel per alpha row is
-    shared by all CTAs (32 <= R < 64), ":cp" for the compact panel (R >= 64)."""
+    shared by all CTAs (32 <= R < 64), ":cp" for the compact panel (R >= 64);
+    ":hs" after the group variant when the beta singles run through hole
+    strings (nt = 0)."""
     key = f"{mode}:{B}" if mode in (6, 7) else str(mode)
+    if mode in (6, 7) and nt == 0:
+        key += ":hs"
     if mode in (1, 3, 6) and R >= 64:
         key += ":cp"
     elif mode in (1, 3, 6) and R >= 32:
@@ -143,11 +151,11 @@ def profile_key(mode, R, B):
     return key
 
 
-def committed_profile(workload, mode, B, R=0):
-    """Per-launch figures of sigma plan (mode, R, B) on `workload` from the
-    committed ncu summary (profiles/sigma_<workload>_traffic.json), or None
-    when that plan was not captured (keys: profile_key)."""
-    key = profile_key(mode, R, B)
+def committed_profile(workload, mode, B, R=0, nt=None):
+    """Per-launch figures of sigma plan (mode, nt, R, B) on `workload` from
+    the committed ncu summary (profiles/sigma_<workload>_traffic.json), or
+    None when that plan was not captured (keys: profile_key)."""
+    key = profile_key(mode, R, B, nt)
     p = os.path.join(ROOT, "profiles", f"sigma_{workload}_traffic.json")
     if os.path.exists(p):
         try:
@@ -576,7 +584,7 @@ def run_gpu(a):
     achieved = bytes_per_launch / avg_launch_s / 1e9
     mode, nt, R, B, tms = sp.sigma_tuning(jb.FP64)
     tune32 = sp.sigma_tuning(jb.FP32)
-    prof = committed_profile(a.workload, mode, B, R) or {}
+    prof = committed_profile(a.workload, mode, B, R, nt) or {}
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": prof.get("dram_bytes_per_launch"),
             "algorithmic_bytes_per_launch": bytes_per_launch, "peak_source": peak_kind,

@@ -36,8 +36,8 @@ def test_every_traffic_entry_points_at_a_committed_summary():
             mode = int(key.split(":")[0])
             assert mode in bench.PLAN_NAMES
             # group plans carry their variant, blocked and shared panels a suffix
-            assert (":" in key.replace(":blk", "").replace(":row", "").replace(":cp", "")) == \
-                (mode in (6, 7))
+            stem = key.replace(":blk", "").replace(":row", "").replace(":cp", "").replace(":hs", "")
+            assert (":" in stem) == (mode in (6, 7))
             assert plan["dram_bytes_per_launch"] > 0 and plan["kernels"]
             assert os.path.exists(os.path.join(bench.ROOT, plan["summary"]))
 
@@ -55,6 +55,8 @@ def test_plan_description_names_each_plans_parameters():
     d = bench.sigma_plan_desc(6, 512, 66, 5)
     assert d["product_ctas_per_sm"] == 2 and "compact" in d["product_panel"]
     assert bench.profile_key(6, 66, 5) == "6:5:cp"
+    assert bench.profile_key(6, 66, 5, 0) == "6:5:hs:cp"
+    assert bench.sigma_plan_desc(6, 0, 66, 5)["beta_singles"] == "hole-string products"
     assert "1 column" in bench.sigma_plan_desc(6, 256, 0, 1)["group_kernel"]
     assert "split over 4 warps, 1 column" in bench.sigma_plan_desc(6, 256, 0, 4)["group_kernel"]
     assert "hole-string" in bench.sigma_plan_desc(6, 256, 0, 5)["group_kernel"]
