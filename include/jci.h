@@ -204,7 +204,8 @@ jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sigma,
  * 5 (4); 6, 7 the same-spin doubles over groups of 16 consecutive strings,
  * the beta singles as a row stream on the transpose, then the product of
  * mode 1 (6) or of mode 5 (7)), threads per CTA of the row kernel (modes
- * 3-4: of the alpha pass; modes 6-7: of the beta-singles stream), `rows`
+ * 3-4: of the alpha pass; modes 6-7: of the beta-singles stream, or 0 for
+ * the beta singles as products over (N-1)-electron hole strings), `rows`
  * (mode 0: alpha rows staged per pass; modes 1-3 and 6: product CTAs per
  * SM, 0 = as many as fit, plus 16 for the panel cut into 256-column blocks
  * gathered block by block, plus 32 for one panel per alpha row built and

@@ -73,6 +73,10 @@ struct FciTables {
     int cp_ent = 0, cp_state = 0;  // cp_state 0 not built, 1 built, -1 not possible
     PairTables prs[2];             // same-spin doubles through hole strings, per spin
     int prs_state = 0;             // 0 not built, 1 built, -1 not possible for this space
+    HsTables hst;                  // beta singles through hole strings
+    int hs_state = 0;              // as prs_state
+    void *hbuf[2] = {nullptr, nullptr};  // their E blocks, per precision
+    size_t hbytes[2] = {0, 0};
     void *pbuf[2] = {nullptr, nullptr};  // their E blocks, per precision
     size_t pbytes[2] = {0, 0};
 };
@@ -124,6 +128,9 @@ void fci_free(DeviceState *d) {
     group_tables_free(&f->grp[1]);
     pair_tables_free(&f->prs[0]);
     pair_tables_free(&f->prs[1]);
+    hs_tables_free(&f->hst);
+    cudaFree(f->hbuf[0]);
+    cudaFree(f->hbuf[1]);
     cudaFree(f->cp_mask);
     cudaFree(f->cp_base);
     cudaFree(f->cp_gidx);
@@ -1425,6 +1432,10 @@ jci_status fci_prepare(jci_space *s) {
             jci_status r = pair_fill(s, &f->prs[sp], st);
             if (r) return r;
         }
+        if (sp == 1 && f->hst.srow) {
+            jci_status r = hs_fill(&f->hst, f->d[1].a1T, f->f[1].a1T, st);
+            if (r) return r;
+        }
     }
     JCI_CUDA(cudaGetLastError());
     return JCI_OK;
@@ -1960,6 +1971,53 @@ static jci_status pair_tables(jci_space *s, cudaStream_t st) {
     return JCI_OK;
 }
 
+// Beta-singles tables through hole strings (jci_fci_pairs.cu), built and
+// filled on first use (not while a stream is being captured); JCI_ERR_SPACE,
+// and remembered, for spaces they do not cover.
+static jci_status hs_tables(jci_space *s, cudaStream_t st) {
+    FciTables *f = s->dev->fci;
+    if (f->hs_state > 0) return JCI_OK;
+    if (f->hs_state < 0) return JCI_ERR_SPACE;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    JCI_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return JCI_ERR_STATE;
+    jci_status r = hs_tables_build(s, 1, &f->hst);
+    if (!r) r = hs_fill(&f->hst, f->d[1].a1T, f->f[1].a1T, st);
+    if (!r && hs_smem_bytes(f->npair, sizeof(double)) > f->smem_max) r = JCI_ERR_SPACE;
+    if (r) {
+        hs_tables_free(&f->hst);
+        f->hs_state = r == JCI_ERR_SPACE ? -1 : 0;
+        return r;
+    }
+    f->hs_state = 1;
+    return JCI_OK;
+}
+
+// The beta singles of plans 6 and 7 with threads = 0: through the hole
+// strings of the beta strings, on C^T (rows Ib) into tau (overwritten).
+template <typename T>
+static jci_status launch_hs(jci_space *s, const StreamArgs<T> &be, const T *ct, T *tau,
+                            cudaStream_t st) {
+    FciTables *f = s->dev->fci;
+    jci_status r = hs_tables(s, st);
+    if (r) return r;
+    const int prec = sizeof(T) == 8 ? 0 : 1;
+    const size_t need =
+        (size_t)f->hst.nk * f->hst.nf * hs_block_cols(f->hst, f->na, sizeof(T)) * sizeof(T);
+    if (f->hbytes[prec] < need) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        JCI_CUDA(cudaStreamIsCapturing(st, &cs));
+        if (cs != cudaStreamCaptureStatusNone) return JCI_ERR_STATE;
+        JCI_CUDA(cudaFree(f->hbuf[prec]));
+        f->hbuf[prec] = nullptr;
+        f->hbytes[prec] = 0;
+        JCI_CUDA(cudaMalloc(&f->hbuf[prec], need));
+        f->hbytes[prec] = need;
+    }
+    return hs_launch<T>(f->hst, f->na, f->npair, be.jc, ct, tau, be.skip, (T *)f->hbuf[prec],
+                        s->dev->device, st);
+}
+
 // E block of the hole-string doubles for variant `items` (5, 6) in this
 // precision, grown on demand (not while a stream is being captured).
 template <typename T>
@@ -2085,7 +2143,8 @@ static jci_status run_plan(jci_space *s, FciArgs<T> a, int mode, int nt, int R, 
         stream_args(a, al, be);
         be.nd = 0;  // the beta doubles come from the group kernel
         if ((r = launch_transposes<T>(f, v, ct, o, tau, false, a.skip, st))) return r;
-        if ((r = launch_stream<T>(be, nt, ct, tau, st))) return r;
+        if ((r = nt == 0 ? launch_hs<T>(s, be, ct, tau, st) : launch_stream<T>(be, nt, ct, tau, st)))
+            return r;
         if ((r = launch_group<T>(s, 1, nullptr, 1, a.skip, B, ct, tau, st))) return r;
         if ((r = launch_group<T>(s, 0, a.hd, 0, a.skip, B, v, o, st))) return r;
         if ((r = launch_transposes<T>(f, v, ct, o, tau, true, a.skip, st))) return r;
@@ -2264,10 +2323,15 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
         stream_args(a, al, be);
         be.nd = 0;
         float bs = 1e30f;
+        bool found = false;
         for (int nt : nts) {
             if (!stream_ok(f->na, nt) || stream_smem(0, be.ns, w) > f->smem_max) continue;
             float ms = timeit([&] { return launch_stream<T>(be, nt, ct, tau, st); });
-            if (ms < bs) { bs = ms; b6s = nt; }
+            if (ms < bs) { bs = ms; b6s = nt; found = true; }
+        }
+        if (hs_tables(s, st) == JCI_OK) {  // threads = 0: the beta singles through hole strings
+            float ms = timeit([&] { return launch_hs<T>(s, be, ct, tau, st); });
+            if (ms < bs) { bs = ms; b6s = 0; found = true; }
         }
         float gg = 1e30f;
         pairs = pair_tables(s, st) == JCI_OK;
@@ -2283,7 +2347,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
             jci_status q = launch_transposes<T>(f, v, ct, o, tau, false, nullptr, st);
             return q ? q : launch_transposes<T>(f, v, ct, o, tau, true, nullptr, st);
         });
-        if (b6s && gg < 1e30f) best6 = bs + gg + tt + bsprod;
+        if (found && gg < 1e30f) best6 = bs + gg + tt + bsprod;
         err = JCI_OK;  // a space the group tables cannot hold just drops the plan
     }
     const int gmode = sab ? 7 : 6;
@@ -2416,9 +2480,9 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, 
     size_t w = p ? sizeof(float) : sizeof(double);
     if (mode == 6 || mode == 7) {
         bool ok = mode == 6 ? mixed_possible(f, w) && R >= 0 : ab_plan_possible(f, R, w);
-        if (!ok || !group_possible(f) || !stream_ok(f->na, nt) || B < 1 || B > 6 ||
-            stream_smem(0, f->sb, w) > f->smem_max)
-            return JCI_ERR_ARG;
+        const bool beta_ok = nt == 0 ? hs_tables(s, s->dev->stream) == JCI_OK
+                                     : stream_ok(f->na, nt) && stream_smem(0, f->sb, w) <= f->smem_max;
+        if (!ok || !group_possible(f) || !beta_ok || B < 1 || B > 6) return JCI_ERR_ARG;
         if (B >= 5 && pair_tables(s, s->dev->stream) != JCI_OK) return JCI_ERR_ARG;
     } else if (mode == 3 || mode == 4) {
         bool ok = mode == 3 ? mixed_possible(f, w) && R >= 0 : ab_plan_possible(f, R, w);

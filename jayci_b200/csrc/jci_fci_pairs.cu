@@ -238,6 +238,88 @@ PairKernel<T> pair_kernel(int RT) {
     }
 }
 
+// ---- singles through (N-1)-electron hole strings ---------------------------
+//
+// Every single I <- J of a one-group space (one electron moved) has exactly
+// one hole string K = I n J with N - 1 electrons; with I = K + k, J = K + l
+// the element is s (a1(K;k,l) + jc[(kl)][c]), the one-body part a1 depending
+// only on K and (k,l) and jc on the column's string of the other spin.  So
+//   E[K][k][c] = sum_{l != k} s_kl (a1_kl + jc[(kl)][c]) X[K + l][c]
+//   Y[I][c]    = sum_{K in I} E[K][I - K][c]            (N rows per string)
+// which reads each source row once per hole string (N - 1 + 1 free orbitals
+// share it) instead of once per single.  Phase 2 is k_pairs_pull.
+constexpr int kHsMaxFree = 16;   // free orbitals of a hole string
+constexpr int kHsPerCta = 32;    // hole strings per CTA of phase 1
+
+template <typename T>
+struct HsArgs {
+    int nk, nf, len, npair;
+    const int *srow;        // [K][x] string K + free orbital x
+    const T *a1s;           // [K][x][y] s (a1 of the single K+x <- K+y), 0 on the diagonal
+    const uint16_t *pp;     // [K][x][y] pair index of the single | phase << 15
+    const T *jc;            // [pair][column] Coulomb part
+    const int *skip;
+};
+
+// Phase 1 for hole strings blockIdx.x * kHsPerCta.. and the 64 columns
+// c0 + 64 blockIdx.y.. of the block [c0, c0 + cb): the jc chunk of every
+// pair is staged in shared memory once per CTA; thread (column, lane)
+// takes every fourth hole string of the CTA.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_hsingles_product(HsArgs<T> a, const T *__restrict__ X, T *__restrict__ E, int c0, int cb) {
+    if (a.skip && *a.skip) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *Js = reinterpret_cast<T *>(smem_raw);  // [npair][64]
+    const int tid = threadIdx.x, col = tid & 63, lane = tid >> 6;
+    const int cc = blockIdx.y * kPairCols + col, c = c0 + cc;
+    const int c1 = min(a.len, c0 + cb);
+    const bool ok = c < c1;
+    for (int idx = tid; idx < a.npair * kPairCols; idx += 256) {
+        const int q = idx >> 6, k = idx & 63, cq = c0 + blockIdx.y * kPairCols + k;
+        Js[idx] = cq < c1 ? a.jc[(long long)q * a.len + cq] : T(0);
+    }
+    __syncthreads();
+    const int nf = a.nf;
+    for (int kk = lane; kk < kHsPerCta; kk += 4) {
+        const int K = blockIdx.x * kHsPerCta + kk;
+        if (K >= a.nk) break;
+        T xv[kHsMaxFree];
+#pragma unroll
+        for (int x = 0; x < kHsMaxFree; x++)
+            xv[x] = (x < nf && ok) ? X[(long long)a.srow[(size_t)K * nf + x] * a.len + c] : T(0);
+        const size_t qb = (size_t)K * nf * nf;
+        for (int x = 0; x < nf; x++) {
+            T acc = T(0);
+#pragma unroll
+            for (int y = 0; y < kHsMaxFree; y++) {
+                if (y >= nf || y == x) continue;
+                const size_t q = qb + x * nf + y;
+                const uint16_t pq = a.pp[q];
+                const T j = Js[(pq & 0x7fff) * kPairCols + col];
+                acc += (a.a1s[q] + ((pq >> 15) ? -j : j)) * xv[y];
+            }
+            if (ok) E[((size_t)K * nf + x) * cb + cc] = acc;
+        }
+    }
+}
+
+// a1s from the current one-body parts: a1s[q] = s a1T[single][string].
+template <typename T>
+__global__ void k_hs_fill(long long n, const int *__restrict__ sidx, const T *__restrict__ a1T,
+                          T *__restrict__ a1s) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int e = sidx[q];
+        T v = T(0);
+        if (e != -1) {
+            v = a1T[e & 0x7fffffff];
+            if (e < 0) v = -v;
+        }
+        a1s[q] = v;
+    }
+}
+
 }  // namespace
 
 // Tables of one spin: the hole strings K (the (N-2)-subsets of the varying
@@ -450,5 +532,192 @@ template jci_status pair_launch<double>(const PairTables &, int, int, const doub
 template jci_status pair_launch<float>(const PairTables &, int, int, const float *, float *,
                                        const float *, int, const int *, float *, int,
                                        cudaStream_t);
+
+// Single tables of one spin through its (N-1)-electron hole strings, in the
+// layout of the pair tables: hole strings in lexical order of the varying
+// orbitals, free orbitals ascending, per string its N - f hole strings in
+// ascending order of the removed orbital.  The coefficient of each ordered
+// free pair (x, y) is the string K + x's single with target K + y (its
+// position in the [single][string] one-body table, its phase, its pair).
+jci_status hs_tables_build(const jci_space *s, int spin, HsTables *t) {
+    const SpinSpace &X = s->sp[spin];
+    const int ns = X.nstr, ne = X.nelec;
+    if (ns < 1 || ne < 1) return JCI_ERR_SPACE;
+    uint64_t uni = 0, all = ~0ull;
+    for (int i = 0; i < ns; i++) {
+        uint64_t m = 0;
+        for (int e = 0; e < ne; e++) {
+            const int o = X.istr[(size_t)i * ne + e];
+            if (o < 1 || o > 64) return JCI_ERR_SPACE;
+            m |= 1ull << (o - 1);
+        }
+        uni |= m;
+        all &= m;
+    }
+    std::vector<int> orb, fixed;
+    for (int o = 1; o <= 64; o++) {
+        if ((all >> (o - 1)) & 1) fixed.push_back(o);
+        else if ((uni >> (o - 1)) & 1) orb.push_back(o);
+    }
+    const int no = (int)orb.size(), nv = ne - (int)fixed.size();
+    if (nv < 1 || no - nv < 1 || binom(no, nv) != ns) return JCI_ERR_SPACE;
+    const int nf = no - nv + 1;
+    if (nf > 16) return JCI_ERR_SPACE;
+    const long long nk = binom(no, nv - 1);
+    if (nk * nf * nf >= (1ll << 31)) return JCI_ERR_SPACE;
+    for (int i = 0; i < ns; i++)
+        if (X.soff[i + 1] - X.soff[i] != (long long)nv * (no - nv)) return JCI_ERR_SPACE;
+    std::vector<uint64_t> kmask;
+    std::unordered_map<uint64_t, int> krank;
+    {
+        std::vector<int> c(nv - 1);
+        for (int i = 0; i < nv - 1; i++) c[i] = i;
+        for (;;) {
+            uint64_t m = 0;
+            for (int x : c) m |= 1ull << x;
+            krank[m] = (int)kmask.size();
+            kmask.push_back(m);
+            int i = nv - 2;
+            while (i >= 0 && c[i] == no - (nv - 1) + i) i--;
+            if (i < 0) break;
+            c[i]++;
+            for (int j = i + 1; j < nv - 1; j++) c[j] = c[j - 1] + 1;
+        }
+    }
+    std::vector<int> srow((size_t)nk * nf), sidx((size_t)nk * nf * nf, -1), pull((size_t)ns * nv);
+    std::vector<uint16_t> pp((size_t)nk * nf * nf, 0);
+    std::vector<int> o(ne), F;
+    for (long long k = 0; k < nk; k++) {
+        const uint64_t m = kmask[k];
+        F.clear();
+        for (int x = 0; x < no; x++)
+            if (!((m >> x) & 1)) F.push_back(x);
+        for (int x = 0; x < nf; x++) {
+            int n = 0;
+            for (int f : fixed) o[n++] = f;
+            for (int y = 0; y < no; y++)
+                if (((m >> y) & 1) || y == F[x]) o[n++] = orb[y];
+            std::sort(o.begin(), o.end());
+            const int I = string_index(s, spin, o.data());
+            if (I < 0) return JCI_ERR_SPACE;
+            srow[(size_t)k * nf + x] = I;
+        }
+        for (int x = 0; x < nf; x++) {
+            const int I = srow[(size_t)k * nf + x];
+            for (int y = 0; y < nf; y++) {
+                if (y == x) continue;
+                const int J = srow[(size_t)k * nf + y];
+                long long f = X.soff[I];
+                while (f < X.soff[I + 1] && X.sing[f].target != J) f++;
+                if (f == X.soff[I + 1]) return JCI_ERR_SPACE;
+                const Exc &e = X.sing[f];
+                const long long pos = (f - X.soff[I]) * ns + I;
+                if (pos >= (1ll << 31) - 1) return JCI_ERR_SPACE;
+                const size_t q = ((size_t)k * nf + x) * nf + y;
+                sidx[q] = (int)pos | (e.sign < 0 ? (int)0x80000000u : 0);
+                const int pr = pair_index(e.io0, e.fo0);
+                if (pr >= 0x8000) return JCI_ERR_SPACE;
+                pp[q] = (uint16_t)(pr | (e.sign < 0 ? 0x8000 : 0));
+            }
+        }
+    }
+    std::vector<int> orbpos(65, -1);
+    for (int x = 0; x < no; x++) orbpos[orb[x]] = x;
+    for (int i = 0; i < ns; i++) {
+        uint64_t m = 0;
+        std::vector<int> vp;
+        for (int e = 0; e < ne; e++) {
+            const int x = orbpos[X.istr[(size_t)i * ne + e]];
+            if (x >= 0) {
+                m |= 1ull << x;
+                vp.push_back(x);
+            }
+        }
+        for (int u = 0; u < nv; u++) {
+            const uint64_t km = m & ~(1ull << vp[u]);
+            const auto it = krank.find(km);
+            if (it == krank.end()) return JCI_ERR_SPACE;
+            int fx = 0;
+            for (int x = 0; x < vp[u]; x++) fx += !((km >> x) & 1);
+            pull[(size_t)i * nv + u] = it->second * nf + fx;
+        }
+    }
+    t->nk = (int)nk; t->nf = nf; t->nt = nv; t->rows = ns;
+    JCI_CUDA(cudaMalloc(&t->srow, srow.size() * sizeof(int)));
+    JCI_CUDA(cudaMalloc(&t->sidx, sidx.size() * sizeof(int)));
+    JCI_CUDA(cudaMalloc(&t->pp, pp.size() * sizeof(uint16_t)));
+    JCI_CUDA(cudaMalloc(&t->pull, pull.size() * sizeof(int)));
+    JCI_CUDA(cudaMalloc(&t->a1s64, sidx.size() * sizeof(double)));
+    JCI_CUDA(cudaMalloc(&t->a1s32, sidx.size() * sizeof(float)));
+    JCI_CUDA(cudaMemcpy(t->srow, srow.data(), srow.size() * sizeof(int), cudaMemcpyHostToDevice));
+    JCI_CUDA(cudaMemcpy(t->sidx, sidx.data(), sidx.size() * sizeof(int), cudaMemcpyHostToDevice));
+    JCI_CUDA(cudaMemcpy(t->pp, pp.data(), pp.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    JCI_CUDA(cudaMemcpy(t->pull, pull.data(), pull.size() * sizeof(int), cudaMemcpyHostToDevice));
+    return JCI_OK;
+}
+
+jci_status hs_fill(HsTables *t, const double *a1T, const float *a1Tf, cudaStream_t st) {
+    const long long n = (long long)t->nk * t->nf * t->nf;
+    const int grid = (int)std::min<long long>((n + 255) / 256, 4096);
+    k_hs_fill<double><<<grid, 256, 0, st>>>(n, t->sidx, a1T, t->a1s64);
+    k_hs_fill<float><<<grid, 256, 0, st>>>(n, t->sidx, a1Tf, t->a1s32);
+    JCI_CUDA(cudaGetLastError());
+    return JCI_OK;
+}
+
+void hs_tables_free(HsTables *t) {
+    cudaFree(t->srow);
+    cudaFree(t->sidx);
+    cudaFree(t->pp);
+    cudaFree(t->pull);
+    cudaFree(t->a1s64);
+    cudaFree(t->a1s32);
+    *t = HsTables();
+}
+
+size_t hs_smem_bytes(int npair, size_t w) { return (size_t)npair * kPairCols * w; }
+
+int hs_block_cols(const HsTables &t, int len, size_t w) {
+    const int full = (len + kPairCols - 1) / kPairCols * kPairCols;
+    const size_t per_col = (size_t)t.nk * t.nf * w;
+    const int cb = (int)std::min<size_t>(full, kPairEBytes / per_col / kPairCols * kPairCols);
+    return std::max(cb, kPairCols);
+}
+
+// Y = the singles of rows x len matrix x (Y overwritten), jc [pair][column]
+// the Coulomb parts, through E blocks of hs_block_cols columns.
+template <typename T>
+jci_status hs_launch(const HsTables &t, int len, int npair, const T *jc, const T *x, T *y,
+                     const int *skip, T *E, int device, cudaStream_t st) {
+    HsArgs<T> a;
+    a.nk = t.nk; a.nf = t.nf; a.len = len; a.npair = npair;
+    a.srow = t.srow; a.pp = t.pp; a.jc = jc; a.skip = skip;
+    if constexpr (sizeof(T) == 8) a.a1s = t.a1s64;
+    else a.a1s = t.a1s32;
+    PairArgs<T> pa{};
+    pa.nk = t.nk; pa.np = t.nf; pa.nt = t.nt; pa.rows = t.rows; pa.len = len;
+    pa.pull = t.pull; pa.skip = skip;
+    const size_t smem = hs_smem_bytes(npair, sizeof(T));
+    int optin = 0;
+    JCI_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    if (smem > (size_t)optin) return JCI_ERR_SPACE;
+    JCI_CUDA(smem_optin(k_hsingles_product<T>));
+    const int cb = hs_block_cols(t, len, sizeof(T));
+    const size_t psmem = (size_t)kPullRows * t.nt * sizeof(int);
+    for (int c0 = 0; c0 < len; c0 += cb) {
+        const int w = std::min(cb, len - c0);
+        dim3 g1((t.nk + kHsPerCta - 1) / kHsPerCta, (w + kPairCols - 1) / kPairCols);
+        k_hsingles_product<T><<<g1, 256, smem, st>>>(a, x, E, c0, cb);
+        dim3 g2((t.rows + kPullRows - 1) / kPullRows, (w + kPairThreads - 1) / kPairThreads);
+        k_pairs_pull<T><<<g2, kPairThreads, psmem, st>>>(pa, E, x, y, nullptr, 0, c0, cb);
+    }
+    JCI_CUDA(cudaGetLastError());
+    return JCI_OK;
+}
+
+template jci_status hs_launch<double>(const HsTables &, int, int, const double *, const double *,
+                                      double *, const int *, double *, int, cudaStream_t);
+template jci_status hs_launch<float>(const HsTables &, int, int, const float *, const float *,
+                                     float *, const int *, float *, int, cudaStream_t);
 
 }  // namespace jci

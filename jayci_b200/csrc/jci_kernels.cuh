@@ -118,6 +118,26 @@ template <typename T>
 jci_status pair_launch(const PairTables &t, int len, int variant, const T *x, T *y, const T *hd,
                        int add, const int *skip, T *E, int device, cudaStream_t st);
 
+// Singles of one spin through (N-1)-electron hole strings, jci_fci_pairs.cu
+// (the beta-singles pass of plans 6 and 7 with threads = 0).
+struct HsTables {
+    int nk = 0, nf = 0, nt = 0, rows = 0;
+    int *srow = nullptr;           // [hole string][free orbital] string
+    int *sidx = nullptr;           // [hole][x][y] one-body table position | phase << 31, -1 diagonal
+    uint16_t *pp = nullptr;        // [hole][x][y] pair | phase << 15
+    int *pull = nullptr;           // [string][hole] hole string * nf + free orbital
+    double *a1s64 = nullptr;       // [hole][x][y] phase x one-body part
+    float *a1s32 = nullptr;
+};
+jci_status hs_tables_build(const jci_space *s, int spin, HsTables *t);
+jci_status hs_fill(HsTables *t, const double *a1T, const float *a1Tf, cudaStream_t st);
+void hs_tables_free(HsTables *t);
+size_t hs_smem_bytes(int npair, size_t w);
+int hs_block_cols(const HsTables &t, int len, size_t w);
+template <typename T>
+jci_status hs_launch(const HsTables &t, int len, int npair, const T *jc, const T *x, T *y,
+                     const int *skip, T *E, int device, cudaStream_t st);
+
 // Generic path (any truncated space), jci_device.cu.
 jci_status device_sigma_generic(jci_space *s, int nvec, const void *vin, void *sout,
                                 long long ld, int precision, cudaStream_t st);

@@ -134,7 +134,9 @@ def test_every_plan_at_fci12(prec):
              # the column-blocked panel (product CTAs per SM + 16)
              (1, 256, 17, 2), (3, 256, 16, 256), (6, 512, 18, 2),
              # the same-spin doubles through hole strings (variants 5, 6)
-             (6, 512, 0, 5), (6, 512, 2, 6), (7, 512, 16, 5)]
+             (6, 512, 0, 5), (6, 512, 2, 6), (7, 512, 16, 5),
+             # the compact panel (+ 64) and the beta singles through hole strings (threads 0)
+             (6, 512, 66, 5), (6, 0, 66, 5), (7, 0, 16, 3)]
     ran = 0
     for plan in plans:
         try:

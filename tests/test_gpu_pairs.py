@@ -1,7 +1,8 @@
 """Same-spin doubles through (N-2)-electron hole strings (jci_fci_pairs.cu,
 group kernel variants 5 and 6 of plans 6 and 7): dense products over the
 free pairs of each hole string, then a pull of the C(N,2) hole rows of every
-string.
+string; and the beta singles through (N-1)-electron hole strings (threads 0
+of plans 6 and 7).
 
 Checked through jci_sigma_device against the reference's own sigma (the
 CAS(10,10) golden vectors, the FCI(12e,12o) rows) and the oracle-pinned rows
@@ -40,7 +41,9 @@ def _sigma(s, v, prec):
 
 @pytest.mark.parametrize("prec", [jb.FP64, jb.FP32])
 @pytest.mark.parametrize("plan", [(6, 256, 0, 5), (6, 256, 0, 6), (7, 256, 16, 5),
-                                  (6, 256, 2, 6)])
+                                  (6, 256, 2, 6),
+                                  # threads 0: the beta singles through hole strings too
+                                  (6, 0, 66, 5), (7, 0, 16, 2), (6, 0, 0, 1)])
 def test_hole_pairs_cas10(plan, prec):
     g = np.load(os.path.join(GOLDEN, "cas10_10.npz"))
     s = jb.Space(*(int(x) for x in g["general"]))
@@ -65,12 +68,13 @@ def test_hole_pairs_with_inactive_orbitals(prec):
     ints = make_integrals(10, 10, 31)
     m1, m2 = ints.packed()
     s.set_integrals(m1, m2, ints.e_nuc, 0.0)
-    s.set_sigma_plan(prec, 6, 128, 0, 5)  # 20 strings per spin: 128-thread streams
     o = OracleSpace(5, 5, 10, ndocc=2, nactv=6)
     v = np.random.default_rng(4).standard_normal(s.ndets)
     ref = o.sigma(m1, m2, v[None, :])[0]
-    y = _sigma(s, v, prec).double().cpu().numpy()
-    assert np.abs(y - ref).max() <= BAR[prec] * np.abs(ref).max()
+    for nt in (128, 0):  # 20 strings per spin: 128-thread streams, or hole-string singles
+        s.set_sigma_plan(prec, 6, nt, 0, 5)
+        y = _sigma(s, v, prec).double().cpu().numpy()
+        assert np.abs(y - ref).max() <= BAR[prec] * np.abs(ref).max(), nt
     s.close()
 
 
@@ -86,8 +90,8 @@ def test_hole_pairs_bench_sizes(name, prec):
     v = hash_vector(s.ndets, int(g["sigma_seed"]))
     rows = torch.from_numpy(g["rows"]).cuda()
     ref = g["sigma_rows"]
-    for variant in (5, 6):
-        s.set_sigma_plan(prec, 6, 512, 2, variant)
+    for nt, variant in ((512, 5), (512, 6), (0, 5)):
+        s.set_sigma_plan(prec, 6, nt, 2, variant)
         y = _sigma(s, v, prec)
         got = y[rows].double().cpu().numpy()
         assert np.abs(got - ref).max() <= BAR[prec] * np.abs(ref).max(), variant
