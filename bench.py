@@ -98,7 +98,8 @@ def sigma_plan_desc(mode, nt, R, B, ms=None):
         d["group_kernel"] = (f"{B} column(s) per thread" if B <= 2 else
                              f"targets split over 4 warps, {5 - B} column(s) per lane" if B <= 4
                              else "hole-string pair products, " +
-                             ("widest column blocks" if B == 5 else "64-column blocks"))
+                             {5: "widest column blocks (1 GiB)", 6: "64-column blocks",
+                              7: "widest column blocks (4 GiB)"}[B])
     else:
         d["beta_pass_threads" if streams else "rows_per_cta"] = B
     if ms is not None:

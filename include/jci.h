@@ -219,8 +219,9 @@ jci_status jci_sigma_device_noalloc(jci_space *s, const void *v, void *sigma,
  * row kernel; modes 3-4: threads per CTA of the beta pass; modes 6-7: the
  * group kernel variant, 1 or 2 columns per thread, or 3, 4: the group's
  * excitation targets split over 4 warps with 2 or 1 columns per lane, or
- * 5, 6: the same-spin doubles as dense products over (N-2)-electron hole
- * strings, in the widest or in 64-column blocks), and
+ * 5-7: the same-spin doubles as dense products over (N-2)-electron hole
+ * strings, in the widest column blocks whose scratch fits 1 GiB (5) or
+ * 4 GiB (7), or in 64-column blocks (6)), and
  * its timed cost in
  * ms per vector.  All 0 before the first sigma call and on the
  * multi-group path.  No reference counterpart (the reference has no device

@@ -2047,8 +2047,8 @@ static jci_status pair_scratch(jci_space *s, int items, cudaStream_t st, T **E) 
 
 // Doubles of spin sp: rows x len matrix x -> y (add: y += ...), with the
 // diagonal hd when given; items = the variant: 1-4 the string-group kernel
-// (group_launch), 5, 6 the hole-string products (pair_launch: widest
-// column block, 64-column blocks).
+// (group_launch), 5-7 the hole-string products (pair_launch: widest column
+// block under 1 GiB of E, 64-column blocks, widest under 4 GiB).
 template <typename T>
 static jci_status launch_group(jci_space *s, int sp, const T *hd, int add, const int *skip,
                                int items, const T *x, T *y, cudaStream_t st) {
@@ -2335,7 +2335,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
         }
         float gg = 1e30f;
         pairs = pair_tables(s, st) == JCI_OK;
-        for (int it : {1, 2, 3, 4, 5, 6}) {
+        for (int it : {1, 2, 3, 4, 5, 6, 7}) {
             if (it >= 5 && !pairs) continue;
             float ms = timeit([&] {
                 jci_status q = launch_group<T>(s, 1, nullptr, 1, nullptr, it, ct, tau, st);
@@ -2370,7 +2370,7 @@ static jci_status autotune(jci_space *s, FciArgs<T> a, cudaStream_t st) {
         // every group kernel variant, end to end (their component timings
         // are close and noisy)
         best6 = 1e30f;
-        for (int it : {1, 2, 3, 4, 5, 6}) {
+        for (int it : {1, 2, 3, 4, 5, 6, 7}) {
             if (it >= 5 && !pairs) continue;
             float ms = best_of([&] { return run_plan<T>(s, a, gmode, b6s, sR, it, v, o, st); });
             if (ms < best6) { best6 = ms; b6i = it; }
@@ -2482,7 +2482,7 @@ jci_status fci_force_plan(jci_space *s, int precision, int mode, int nt, int R, 
         bool ok = mode == 6 ? mixed_possible(f, w) && R >= 0 : ab_plan_possible(f, R, w);
         const bool beta_ok = nt == 0 ? hs_tables(s, s->dev->stream) == JCI_OK
                                      : stream_ok(f->na, nt) && stream_smem(0, f->sb, w) <= f->smem_max;
-        if (!ok || !group_possible(f) || !beta_ok || B < 1 || B > 6) return JCI_ERR_ARG;
+        if (!ok || !group_possible(f) || !beta_ok || B < 1 || B > 7) return JCI_ERR_ARG;
         if (B >= 5 && pair_tables(s, s->dev->stream) != JCI_OK) return JCI_ERR_ARG;
     } else if (mode == 3 || mode == 4) {
         bool ok = mode == 3 ? mixed_possible(f, w) && R >= 0 : ab_plan_possible(f, R, w);

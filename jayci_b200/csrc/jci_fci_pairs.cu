@@ -35,6 +35,7 @@ constexpr int kPairThreads = 256;
 constexpr int kPairCols = 64;      // columns per staged chunk
 constexpr int kPullRows = 8;       // strings per CTA of the pull
 constexpr size_t kPairEBytes = size_t(1) << 30;  // E of the widest column block
+constexpr size_t kPairEBytesWide = size_t(4) << 30;  // the same for variant 7
 
 template <typename T>
 struct PairArgs {
@@ -487,13 +488,14 @@ size_t pair_smem_bytes(const PairTables &t, int prec) {
 }
 
 // Columns per block of phase 1 / phase 2: variant 5 the widest block whose E
-// fits kPairEBytes, variant 6 one 64-column chunk (E small enough for L2 at
-// the mid sizes).
+// fits kPairEBytes (variant 7: kPairEBytesWide, fewer launches and W_K
+// builds for more memory), variant 6 one 64-column chunk (E small enough
+// for L2 at the mid sizes).
 int pair_block_cols(const PairTables &t, int len, int variant, size_t w) {
     const int full = (len + kPairCols - 1) / kPairCols * kPairCols;
     if (variant == 6) return kPairCols;
     const size_t per_col = (size_t)t.nk * t.np * w;
-    const int cb = (int)std::min<size_t>(full, kPairEBytes / per_col / kPairCols * kPairCols);
+    const int cb = (int)std::min<size_t>(full, (variant == 7 ? kPairEBytesWide : kPairEBytes) / per_col / kPairCols * kPairCols);
     return std::max(cb, kPairCols);
 }
 

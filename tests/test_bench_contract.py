@@ -60,6 +60,7 @@ def test_plan_description_names_each_plans_parameters():
     assert "1 column" in bench.sigma_plan_desc(6, 256, 0, 1)["group_kernel"]
     assert "split over 4 warps, 1 column" in bench.sigma_plan_desc(6, 256, 0, 4)["group_kernel"]
     assert "hole-string" in bench.sigma_plan_desc(6, 256, 0, 5)["group_kernel"]
+    assert "4 GiB" in bench.sigma_plan_desc(6, 256, 0, 7)["group_kernel"]
     assert "64-column" in bench.sigma_plan_desc(7, 256, 16, 6)["group_kernel"]
     d = bench.sigma_plan_desc(3, 256, 0, 512)
     assert d["alpha_pass_threads"] == 256 and d["beta_pass_threads"] == 512

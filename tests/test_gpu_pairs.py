@@ -90,7 +90,7 @@ def test_hole_pairs_bench_sizes(name, prec):
     v = hash_vector(s.ndets, int(g["sigma_seed"]))
     rows = torch.from_numpy(g["rows"]).cuda()
     ref = g["sigma_rows"]
-    for nt, variant in ((512, 5), (512, 6), (0, 5)):
+    for nt, variant in ((512, 5), (512, 6), (0, 5), (512, 7)):
         s.set_sigma_plan(prec, 6, nt, 2, variant)
         y = _sigma(s, v, prec)
         got = y[rows].double().cpu().numpy()

@@ -138,7 +138,9 @@ def test_noalloc_first_call_allocates_nothing(n, prec):
 # shape whatever plan the space was left with
 PLANS = [(0, 128, 2, 1), (0, 512, 4, 1), (1, 128, 0, 1), (1, 1024, 0, 1), (2, 256, 0, 2),
          (3, 128, 0, 1024), (3, 1024, 0, 128), (4, 512, 16, 512), (5, 256, 8, 1),
-         (6, 128, 0, 2), (6, 1024, 0, 1), (7, 512, 16, 3), (7, 128, 8, 4)]
+         (6, 128, 0, 2), (6, 1024, 0, 1), (7, 512, 16, 3), (7, 128, 8, 4),
+         # compact panel, hole-string doubles (5, 6) and beta singles (threads 0)
+         (6, 512, 66, 5), (6, 0, 68, 6), (7, 0, 16, 5)]
 
 
 @pytest.mark.parametrize("prec", [jb.FP64, jb.FP32])
