@@ -159,8 +159,9 @@ jci_status jci_sigma(jci_space *s, int nvec, const double *v, double *sigma,
 
 /* Same on device memory: nvec vectors with leading dimension ld (>= ndets,
  * elements); element type double for JCI_FP64, float for JCI_FP32.  The
- * work is queued on `stream` (a cudaStream_t; NULL = the handle's own
- * stream, not the legacy default stream). */
+ * work is queued on `stream` (a cudaStream_t).  NULL = the handle's own
+ * stream, ordered after the work already queued on the legacy default
+ * stream, which in turn waits for the sigma before its later work. */
 jci_status jci_sigma_device(jci_space *s, int nvec, const void *v,
                             void *sigma, long long ld, int precision,
                             void *stream);

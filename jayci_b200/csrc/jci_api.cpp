@@ -83,7 +83,18 @@ jci_status jci_sigma_device(jci_space *s, int nvec, const void *v, void *sig, lo
                             int precision, void *stream) {
     if (!s) return JCI_ERR_ARG;
     if (precision != JCI_FP64 && precision != JCI_FP32) return JCI_ERR_ARG;
-    return device_sigma(s, nvec, v, sig, ld, precision, stream);
+    if (stream || !s->dev) return device_sigma(s, nvec, v, sig, ld, precision, stream);
+    // NULL stream: the handle's stream, after the work the caller queued on
+    // the legacy default stream (its inputs and outputs are often written
+    // there), and that stream waits for the sigma
+    DeviceState *d = s->dev;
+    JCI_CUDA(cudaEventRecord(d->evin, cudaStreamLegacy));
+    JCI_CUDA(cudaStreamWaitEvent(d->stream, d->evin, 0));
+    jci_status r = device_sigma(s, nvec, v, sig, ld, precision, nullptr);
+    if (r) return r;
+    JCI_CUDA(cudaEventRecord(d->evout, d->stream));
+    JCI_CUDA(cudaStreamWaitEvent(cudaStreamLegacy, d->evout, 0));
+    return JCI_OK;
 }
 
 jci_status jci_sigma(jci_space *s, int nvec, const double *v, double *sig, int precision) {

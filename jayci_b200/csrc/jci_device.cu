@@ -78,6 +78,8 @@ jci_status device_init(jci_space *s) {
     JCI_CUDA(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
     JCI_CUDA(cudaEventCreate(&d->ev0));
     JCI_CUDA(cudaEventCreate(&d->ev1));
+    JCI_CUDA(cudaEventCreateWithFlags(&d->evin, cudaEventDisableTiming));
+    JCI_CUDA(cudaEventCreateWithFlags(&d->evout, cudaEventDisableTiming));
     d->norb = s->ci_orbs;
     d->npair = s->ci_orbs * (s->ci_orbs + 1) / 2;
     d->npq = s->npq;
@@ -173,6 +175,8 @@ void device_free(jci_space *s) {
     davidson_free(d);
     if (d->ev0) cudaEventDestroy(d->ev0);
     if (d->ev1) cudaEventDestroy(d->ev1);
+    if (d->evin) cudaEventDestroy(d->evin);
+    if (d->evout) cudaEventDestroy(d->evout);
     if (d->stream) cudaStreamDestroy(d->stream);
     delete d;
     s->dev = nullptr;

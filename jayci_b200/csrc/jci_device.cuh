@@ -64,6 +64,7 @@ struct DeviceState {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t evin = nullptr, evout = nullptr;  // ordering with the legacy default stream
     float last_sigma_ms = 0.f;
     SpinTables t[2];
     int npq = 0;

@@ -95,7 +95,10 @@ def test_hole_pairs_bench_sizes(name, prec):
         y = _sigma(s, v, prec)
         got = y[rows].double().cpu().numpy()
         assert np.abs(got - ref).max() <= BAR[prec] * np.abs(ref).max(), variant
-        assert torch.equal(_sigma(s, v, prec), y)
+        y2 = _sigma(s, v, prec)
+        diff = (y2 != y).sum().item()
+        assert diff == 0, (nt, variant, diff, torch.isnan(y).sum().item(),
+                           torch.isnan(y2).sum().item(), (y2 - y).abs().max().item())
     s.close()
 
 
